@@ -1,0 +1,366 @@
+"""Benchmark: 2DES propagations/sec on the 1024-point dimer delay scan.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one pass over the whole scan): the dimer of the c0 fixture
+(N = 4 levels, 70 ADOs) scanned over 64 t1 delays (0-315 fs) x 8 waiting times
+(0-700 fs) x {rephasing, non-rephasing} = 1024 independent 2DES points, t3 = 400 fs,
+dt = 0.5 fs (901-2931 RK4 steps per point).  One propagation = one point = the three
+mask trajectories 111, 110, 101 combined, as one CPU_2DES run of one key file.
+
+value: propagations/s of the chosen path (batched FP32-bulk scan kernel, inputs resident
+on the device, CUDA-event time of the scan graph per step, L2 flushed between steps).
+e2e:   the same through the public C ABI with host buffers (heom_run_scan: H2D of the
+points, D2H of every P(t)), wall time of the synchronous call.
+Also reported: the plain FP64 path (bit-exact, one point at a time) on a sample of
+points, the FP32-bulk error against the FP64 scan, the roofline of the scan kernel,
+GPU clocks during the timed region and the reference CPU build on a bounded sample.
+
+Multi-GPU (torchrun): every rank runs its own 1024-point scan (a different disorder
+sample), no collective on the data path; value = all points / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+
+METRIC = "2DES propagations/sec, chosen vs plain FP64 on 1 B200 at ≤1e-6 P(t) err"
+UNIT = "propagations/s"
+KEY = os.path.join(ROOT, "tests", "golden", "keys", "c0_dimer.key")
+TEMPLATE = os.path.join(ROOT, "tests", "golden", "keys", "c2_dimer_scan.key-tmpl")
+
+
+def scan_rows():
+    from make_fixtures import scan_points
+    return [(a, b, c, d) for a, b, c, d, _ in scan_points()]
+
+
+def flops_per_traj_step(N: int, n_ado: int, links: int) -> float:
+    """Algorithmic real flops of one RK4 step of one trajectory: four stages of the
+    dense commutator (16 N^3), damping + stage axpys (24 N^2) per ADO and one-hot
+    row/column neighbour updates (16 N per link)."""
+    return 4.0 * (n_ado * (16 * N ** 3 + 24 * N ** 2) + 16 * N * links)
+
+
+def steps_of(t_end: float, t_start: float = 0.0, dt: float = 0.5) -> int:
+    nstep = np.float32((np.float32(t_end) - np.float32(t_start)) / np.float32(dt))
+    return int(nstep) + 1 if nstep >= 0 else 0
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        busy = [s for s in sm if mx and s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def fp32_peak_tflops(heom, device: int) -> float:
+    """FP32 FMA throughput of this GPU, measured now by the library's FMA-loop kernel
+    (best of three); the scan kernel runs on these pipes, not on the tensor cores."""
+    return max(heom.fma_peak_tflops(device, fp64=False) for _ in range(3))
+
+
+# ------------------------------------------------------------------ reference arm
+def reference_cpu(rows, n_points: int, cores: int):
+    """Run the reference's own CPU build (oracle/_ref/CPU_2DES, one process per key file,
+    `cores` at a time -- the reference's process-per-key model) on n_points points."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "CPU_2DES")
+    kind = "reference"
+    if not os.path.exists(exe):
+        exe = os.path.join(ROOT, "oracle", "heom_oracle")
+        kind = "port"
+        if not os.path.exists(exe):
+            subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "all"])
+    tmpl = open(TEMPLATE).read()
+    # stratified sample: spread over the scan
+    idx = np.linspace(0, len(rows) - 1, n_points).round().astype(int)
+    d = tempfile.mkdtemp()
+    keys = []
+    for j, i in enumerate(idx):
+        r = rows[i]
+        t = (tmpl.replace("TAU1", repr(r[0])).replace("TAU2", repr(r[1])).replace("TAU3", repr(r[2]))
+             .replace("T_END", repr(r[3])))
+        p = os.path.join(d, f"key_{j}.key")
+        open(p, "w").write(t)
+        keys.append(p)
+    t0 = time.perf_counter()
+    procs = []
+    for p in keys:
+        while len([q for q in procs if q.poll() is None]) >= cores:
+            time.sleep(0.005)
+        procs.append(subprocess.Popen([exe, p] + (["--structured"] if kind == "port" else []),
+                                      stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
+    for q in procs:
+        q.wait()
+    wall = time.perf_counter() - t0
+    shutil.rmtree(d, ignore_errors=True)
+    steps = sum(steps_of(rows[i][3]) for i in idx)
+    return len(keys) / wall, kind, wall, steps
+
+
+def run_reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    rows = scan_rows()
+    cores = os.cpu_count() or 1
+    per_step = max(cores, 1)
+    vals = []
+    kind = "reference"
+    wall_total = 0.0
+    for s in range(a.warmup + a.steps):
+        v, kind, wall, _ = reference_cpu(rows, per_step, cores)
+        if s >= a.warmup:
+            vals.append(v)
+            wall_total += wall
+    value = float(np.mean(vals))
+    sample = (f"{per_step} stratified scan points per step, one CPU_2DES process per key file, "
+              f"{cores} concurrent (the reference's process-per-key model)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * wall_total / max(a.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": "c2 dimer 2DES delay scan (1024 points), reference CPU build",
+                                        "points_per_step": per_step},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(a):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from heomtest import load_pkg, rel_err
+
+    heom = load_pkg()
+    prob = heom.Problem.from_key(KEY)
+    for _ in range(rank + 1):  # each rank: its own disorder/orientation sample
+        prob.prepare_sample()
+    rows = scan_rows()
+    n = len(rows)
+    pts = heom.make_points(rows)
+    plan = heom.Plan(prob, "fp32-bulk", device=local, max_points=n, autotune=True)
+    pts, off, cnt, tot = plan.scan_layout(pts)
+
+    # device-resident inputs
+    d_pts = torch.from_numpy(pts.view(np.uint8).copy()).cuda()
+    d_off = torch.from_numpy(off.copy()).cuda()
+    d_P = torch.zeros(2 * tot, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
+    stream = torch.cuda.current_stream()
+
+    def one_scan():
+        plan.run_scan_device(d_pts.data_ptr(), n, d_P.data_ptr(), d_off.data_ptr())
+
+    # The plan runs on its own stream; bracket every scan with events on that stream by
+    # synchronising around it (the scan is ~0.1 s, the host gap is negligible).
+    for _ in range(a.warmup):
+        one_scan()
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = plan.launches
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            one_scan()
+            torch.cuda.synchronize()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+    launches = plan.launches - launches0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = float(np.mean(times))
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n / (ms / 1e3)
+
+    # kernel-only duration (CUDA events around the scan kernel alone are the same
+    # graph; the order kernel is ~10 us), roofline of the scan kernel
+    inf = prob.info
+    depth = prob.ado().astype(int).sum(axis=1)
+    up_links = int((depth < inf.L).sum() * inf.K * inf.K_m)  # down links are equal in number
+    F = flops_per_traj_step(inf.sys_size, inf.n_ado, 2 * up_links)
+    traj_steps = 3 * sum(steps_of(r[3]) for r in rows)
+    alg_flops = F * traj_steps
+    achieved = alg_flops / (ms / 1e3) / 1e12
+    peak = fp32_peak_tflops(heom, local)
+
+    out = None
+    if rank == 0:
+        # e2e through the host-buffer C ABI
+        e2e_t = []
+        for s in range(max(2, min(a.steps, 5))):
+            t0 = time.perf_counter()
+            r32 = plan.run_scan(pts, (pts, off, cnt, tot))
+            e2e_t.append(time.perf_counter() - t0)
+        e2e_val = n / float(np.mean(e2e_t[1:] if len(e2e_t) > 1 else e2e_t))
+        # accuracy gate: FP32-bulk vs the FP64 scan path on the full scan
+        r64 = heom.Plan(prob, "fp64", device=local, max_points=n).run_scan(pts, (pts, off, cnt, tot))
+        errs = [rel_err(r32.point(i), r64.point(i)) for i in range(n)]
+        # plain FP64 path (bit-exact, one point at a time) on a stratified sample
+        tmpl = open(TEMPLATE).read()
+        sample_idx = np.linspace(0, n - 1, 8).round().astype(int)
+        plain_t, plain_steps = 0.0, 0
+        tmpd = tempfile.mkdtemp()
+        for i in sample_idx:
+            r = rows[i]
+            k = os.path.join(tmpd, "p.key")
+            open(k, "w").write(tmpl.replace("TAU1", repr(r[0])).replace("TAU2", repr(r[1]))
+                               .replace("TAU3", repr(r[2])).replace("T_END", repr(r[3])))
+            pp = heom.Problem.from_key(k)
+            pp.prepare_sample()
+            pl = heom.Plan(pp, "fp64-exact", device=local)
+            pl.run_2des()  # warm
+            t0 = time.perf_counter()
+            pl.run_2des()
+            plain_t += time.perf_counter() - t0
+            plain_steps += steps_of(r[3])
+            pl.close()
+        shutil.rmtree(tmpd, ignore_errors=True)
+        # scale the sample to the whole scan by step count
+        full_steps = sum(steps_of(r[3]) for r in rows)
+        plain_val = n / (plain_t * full_steps / plain_steps)
+        # CPU baseline: the reference build on a bounded sample
+        cores = os.cpu_count() or 1
+        cpu_val, kind, wall, _ = reference_cpu(rows, cores, cores)
+        clocks = clk.summary()
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 contractions / f64 state", "data": "synthetic",
+            "config": {"workload": "c2: 1024-point dimer 2DES delay scan (64 t1 x 8 t2 x R/NR, t3 400 fs, "
+                                   "dt 0.5 fs, N=4, 70 ADOs), batched FP32-bulk scan kernel",
+                       "points_per_gpu": n, "rk4_steps_per_point": [min(steps_of(r[3]) for r in rows),
+                                                                    max(steps_of(r[3]) for r in rows)],
+                       "l2": "flushed (256 MB write) between timed steps; state is shared-memory resident",
+                       "launch": plan.describe(), "parallelism": f"dp{world} (independent scans)"},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(pts.nbytes + off.nbytes),
+                    "d2h_bytes_per_step": int(16 * tot)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": ("algorithmic flops = 3 trajectories x RK4 steps x "
+                                  f"{F:.0f} flop/step (4 stages: 16N^3 + 24N^2 per ADO, 16N per link); "
+                                  "peak = FP32 FMA throughput measured in this run by the library's "
+                                  "FMA-loop kernel (MEASURED_PEAKS.json holds only HBM and bf16 tensor peaks)")},
+            "accuracy": {"fp32_bulk_vs_fp64_max_rel_err": float(max(errs)),
+                         "fp32_bulk_vs_fp64_median_rel_err": float(np.median(errs)), "points_checked": n},
+            "plain_fp64": {"value": plain_val, "unit": UNIT, "sample": f"{len(sample_idx)} points, one at a time, "
+                           "bit-exact FP64 path, scaled to the scan by RK4 step count",
+                           "speedup_of_chosen": value / plain_val},
+            "cpu_baseline": {"value": cpu_val, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": f"{cores} stratified scan points, one CPU_2DES process each, "
+                                       f"{cores} concurrent ({wall:.1f} s)"},
+            "clocks": clocks,
+        }
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    a = ap.parse_args()
+    if a.impl == "reference":
+        run_reference_arm(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

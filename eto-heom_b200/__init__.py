@@ -1,0 +1,265 @@
+"""Python face of the B200 HEOM-ETO 2DES propagation library (libheom.so, C ABI).
+
+Mirrors the reference's solver interface (etoheom-cpu/lib/dynamics.h:19-25,
+param.h:38-82) over the C ABI declared in include/heom.h:
+
+    prob = Problem.from_key("key.key")        # param::param_2des + construct_ADO_set
+    prob.prepare_sample()                      # construct_Hal + polar_mat_ranrot + ...
+    plan = Plan(prob, precision="fp64-exact")  # device plan
+    P = plan.run_traj(1, 1, 0)                 # twoD_spectrum_solver(key, H, 1, 1, 0, P)
+    P, trajs = plan.run_2des()                 # CPU_2DES's p111 - p110 - p101
+    P = plan.run_scan(points)                  # a whole delay scan in one launch
+
+There is no CPU fallback: every propagation runs in the CUDA kernels of libheom.so,
+and constructing a Plan without a CUDA device raises HeomError.  The package
+directory name contains a hyphen, so load it by path (see load_package()).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libheom.so")
+
+FP64_EXACT, FP64, FP32_BULK = 0, 1, 2
+PRECISIONS = {"fp64-exact": FP64_EXACT, "fp64": FP64, "fp32-bulk": FP32_BULK}
+MAT_H, MAT_X0, MAT_X1, MAT_X2, MAT_X3, MAT_HKEY = range(6)
+KEY_SINGLE_MANIFOLD = 1
+
+ERRORS = {-1: "argument", -2: "io", -3: "parse", -4: "cuda", -5: "nomem", -6: "capacity",
+          -7: "unsupported", -8: "numeric", -9: "timeout"}
+
+
+class HeomError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)} error ({code}): {msg}")
+        self.code = code
+
+
+class ProblemInfo(ctypes.Structure):
+    _fields_ = [("single_size", ctypes.c_int), ("sys_size", ctypes.c_int), ("K", ctypes.c_int),
+                ("K_m", ctypes.c_int), ("L", ctypes.c_int), ("n_ado", ctypes.c_int),
+                ("n_sample", ctypes.c_int), ("seed", ctypes.c_ulong), ("n_steps", ctypes.c_int),
+                ("print_stride", ctypes.c_int), ("n_record", ctypes.c_int),
+                ("t_start", ctypes.c_float), ("t_end", ctypes.c_float), ("step_size", ctypes.c_float),
+                ("print_step", ctypes.c_float), ("E0", ctypes.c_double * 3), ("tau", ctypes.c_double * 3),
+                ("taup", ctypes.c_double * 3), ("w0", ctypes.c_double * 3)]
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("device", ctypes.c_int), ("stream", ctypes.c_void_p),
+                ("max_points", ctypes.c_int), ("autotune", ctypes.c_int)]
+
+
+class ScanPoint(ctypes.Structure):
+    _fields_ = [("tau1", ctypes.c_double), ("tau2", ctypes.c_double), ("tau3", ctypes.c_double),
+                ("t_end", ctypes.c_float), ("flags", ctypes.c_int)]
+
+
+SCAN_POINT_DTYPE = np.dtype([("tau1", "<f8"), ("tau2", "<f8"), ("tau3", "<f8"), ("t_end", "<f4"),
+                             ("flags", "<i4")])
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libheom.so once; raise (never fall back) if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise HeomError(-4, f"{LIB_PATH} is not built; run eto-heom_b200/build.py")
+    L = ctypes.CDLL(LIB_PATH)
+    P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "heom_last_error": (ctypes.c_char_p, []),
+        "heom_abi_version": (I, []),
+        "heom_problem_from_key": (I, [ctypes.c_char_p, I, ctypes.POINTER(P)]),
+        "heom_problem_info_get": (I, [P, ctypes.POINTER(ProblemInfo)]),
+        "heom_problem_prepare_sample": (I, [P]),
+        "heom_problem_prepare_identity": (I, [P]),
+        "heom_problem_reset_rng": (I, [P]),
+        "heom_problem_get_matrix": (I, [P, I, D]),
+        "heom_problem_set_matrix": (I, [P, I, D]),
+        "heom_problem_get_ado": (I, [P, ctypes.POINTER(ctypes.c_ubyte)]),
+        "heom_problem_destroy": (None, [P]),
+        "heom_plan_create": (I, [P, ctypes.POINTER(Opts), ctypes.POINTER(P)]),
+        "heom_plan_update": (I, [P, P]),
+        "heom_run_traj": (I, [P, I, I, I, D, I, ctypes.POINTER(I)]),
+        "heom_run_2des": (I, [P, D, D, I, ctypes.POINTER(I)]),
+        "heom_scan_layout": (I, [P, P, I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(I),
+                                 ctypes.POINTER(ctypes.c_longlong)]),
+        "heom_run_scan": (I, [P, P, I, D, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(I)]),
+        "heom_run_scan_device": (I, [P, P, I, P, P]),
+        "heom_plan_describe": (I, [P, ctypes.c_char_p, I]),
+        "heom_plan_launch_count": (ctypes.c_longlong, [P]),
+        "heom_plan_destroy": (None, [P]),
+        "heom_measure_fma_peak": (I, [I, I, D]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise HeomError(rc, lib().heom_last_error().decode())
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Problem:
+    """A parsed key file plus its current disorder/orientation sample."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def from_key(cls, path: str, single_manifold: bool = False) -> "Problem":
+        h = ctypes.c_void_p()
+        _check(lib().heom_problem_from_key(os.fsencode(path), KEY_SINGLE_MANIFOLD if single_manifold else 0,
+                                           ctypes.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.heom_problem_destroy(self._h)
+            self._h = None
+
+    @property
+    def info(self) -> ProblemInfo:
+        inf = ProblemInfo()
+        _check(lib().heom_problem_info_get(self._h, ctypes.byref(inf)))
+        return inf
+
+    def prepare_sample(self) -> None:
+        _check(lib().heom_problem_prepare_sample(self._h))
+
+    def prepare_identity(self) -> None:
+        _check(lib().heom_problem_prepare_identity(self._h))
+
+    def reset_rng(self) -> None:
+        _check(lib().heom_problem_reset_rng(self._h))
+
+    def matrix(self, which: int) -> np.ndarray:
+        N = self.info.sys_size
+        out = np.zeros((N, N), dtype=np.complex128)
+        _check(lib().heom_problem_get_matrix(self._h, which, _dptr(out)))
+        return out
+
+    def set_matrix(self, which: int, m: np.ndarray) -> None:
+        a = np.ascontiguousarray(m, dtype=np.complex128)
+        _check(lib().heom_problem_set_matrix(self._h, which, _dptr(a)))
+
+    def ado(self) -> np.ndarray:
+        inf = self.info
+        out = np.zeros((inf.n_ado, inf.K * inf.K_m), dtype=np.uint8)
+        _check(lib().heom_problem_get_ado(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte))))
+        return out
+
+
+@dataclass
+class ScanResult:
+    P: np.ndarray          # concatenated complex points
+    offsets: np.ndarray    # int64 per point
+    counts: np.ndarray     # int32 per point
+
+    def point(self, i: int) -> np.ndarray:
+        return self.P[self.offsets[i]:self.offsets[i] + self.counts[i]]
+
+
+class Plan:
+    """A device plan for one problem (one CUDA device and stream)."""
+
+    def __init__(self, problem: Problem, precision="fp64-exact", device: int = 0, max_points: int = 1024,
+                 autotune: bool = False, stream: int | None = None):
+        self.problem = problem
+        prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        o = Opts(prec, device, ctypes.c_void_p(stream) if stream else None, max_points, 1 if autotune else 0)
+        h = ctypes.c_void_p()
+        _check(lib().heom_plan_create(problem._h, ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self.precision = prec
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.heom_plan_destroy(self._h)
+            self._h = None
+
+    def close(self) -> None:
+        self.__del__()
+
+    def update(self) -> None:
+        _check(lib().heom_plan_update(self._h, self.problem._h))
+
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(512)
+        _check(lib().heom_plan_describe(self._h, buf, 512))
+        return buf.value.decode()
+
+    @property
+    def launches(self) -> int:
+        return int(lib().heom_plan_launch_count(self._h))
+
+    def run_traj(self, nv1: int, nv2: int, nv3: int) -> np.ndarray:
+        cap = max(self.problem.info.n_record, 1)
+        out = np.zeros(cap, dtype=np.complex128)
+        n = ctypes.c_int()
+        _check(lib().heom_run_traj(self._h, nv1, nv2, nv3, _dptr(out), cap, ctypes.byref(n)))
+        return out[:n.value]
+
+    def run_2des(self):
+        cap = max(self.problem.info.n_record, 1)
+        P = np.zeros(cap, dtype=np.complex128)
+        tr = np.zeros((3, cap), dtype=np.complex128)
+        n = ctypes.c_int()
+        _check(lib().heom_run_2des(self._h, _dptr(P), _dptr(tr), cap, ctypes.byref(n)))
+        return P[:n.value], tr[:, :n.value]
+
+    def scan_layout(self, points: np.ndarray):
+        pts = np.ascontiguousarray(points, dtype=SCAN_POINT_DTYPE)
+        n = len(pts)
+        off = np.zeros(n, dtype=np.int64)
+        cnt = np.zeros(n, dtype=np.int32)
+        tot = ctypes.c_longlong()
+        _check(lib().heom_scan_layout(self._h, pts.ctypes.data_as(ctypes.c_void_p), n,
+                                      off.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+                                      cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(tot)))
+        return pts, off, cnt, int(tot.value)
+
+    def run_scan(self, points: np.ndarray, layout=None) -> ScanResult:
+        pts, off, cnt, tot = layout if layout is not None else self.scan_layout(points)
+        P = np.zeros(max(tot, 1), dtype=np.complex128)
+        _check(lib().heom_run_scan(self._h, pts.ctypes.data_as(ctypes.c_void_p), len(pts), _dptr(P),
+                                   off.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+                                   cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        return ScanResult(P[:tot], off, cnt)
+
+    def run_scan_device(self, d_pts: int, n: int, d_P: int, d_offsets: int) -> None:
+        """Device-pointer form (e.g. torch tensors' data_ptr()); asynchronous on the plan's stream."""
+        _check(lib().heom_run_scan_device(self._h, ctypes.c_void_p(d_pts), n, ctypes.c_void_p(d_P),
+                                          ctypes.c_void_p(d_offsets)))
+
+
+def fma_peak_tflops(device: int = 0, fp64: bool = False) -> float:
+    """Measured FP32/FP64 FMA throughput of a device (TFLOP/s)."""
+    v = ctypes.c_double()
+    _check(lib().heom_measure_fma_peak(device, 1 if fp64 else 0, ctypes.byref(v)))
+    return float(v.value)
+
+
+def make_points(rows) -> np.ndarray:
+    """Scan points from (tau1, tau2, tau3, t_end) rows."""
+    pts = np.zeros(len(rows), dtype=SCAN_POINT_DTYPE)
+    for i, r in enumerate(rows):
+        pts[i] = (r[0], r[1], r[2], r[3], 0)
+    return pts

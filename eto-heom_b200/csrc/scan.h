@@ -1,0 +1,58 @@
+// Batched 2DES delay-scan path (HEOM_FP64 / HEOM_FP32_BULK): host state and entry points.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/heom.h"
+#include "heom_host.h"
+
+namespace heom_dev {
+
+struct ScanState {
+  int precision = HEOM_FP32_BULK;
+  int N = 0, n_ado = 0, M = 0, K = 0, K_m = 0, E = 0, max_points = 0;
+  bool supported = false;
+  std::string why;
+  // launch shape (autotuned)
+  int ept = 8, threads = 0, grid = 0, sm_count = 0;
+  size_t smem = 0;
+  float tune_ms = 0;
+  // problem constants
+  float t_start = 0, dt = 0;
+  int stride = 1;
+  double E0[3] = {0, 0, 0}, taup[3] = {0, 0, 0}, w0[3] = {0, 0, 0}, h = 0;
+  // device buffers
+  void *d_tables = nullptr;      // packed read-only tables (see scan.cu)
+  size_t tables_bytes = 0;
+  double *d_sys = nullptr;       // Hd, Hoff, Xs, X3 (re-uploaded per sample)
+  size_t sys_doubles = 0;
+  heom_scan_point *d_pts = nullptr;
+  long long *d_offsets = nullptr;
+  double *d_P = nullptr;
+  long long P_cap = 0;
+  int *d_order = nullptr, *d_counter = nullptr, *d_status = nullptr;
+  // pinned staging for the host-buffer entry point
+  heom_scan_point *h_pts = nullptr;
+  long long *h_offsets = nullptr;
+  double *h_P = nullptr;
+  long long hP_cap = 0;
+  // graph cache for heom_run_scan_device
+  cudaGraphExec_t gexec = nullptr;
+  const void *g_key[4] = {nullptr, nullptr, nullptr, nullptr};
+  int g_n = -1;
+};
+
+int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_points, bool autotune, cudaStream_t st);
+int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st);
+int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, const long long *offsets,
+                  long long total, cudaStream_t st);
+int scan_run_device(ScanState &s, const heom_scan_point *d_pts, int n, double *d_P, const long long *d_offsets,
+                    cudaStream_t st);
+void scan_release(ScanState &s);
+std::string scan_describe(const ScanState &s);
+const char *scan_last_error();
+long long scan_launches_per_run(const ScanState &s);
+
+} // namespace heom_dev

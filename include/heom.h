@@ -1,0 +1,150 @@
+/* heom.h -- C ABI of the B200-native HEOM-ETO 2DES propagation library (libheom.so).
+ *
+ * Drop-in for the propagation path of KaiChengLiu/ETO-HEOM.  The reference exposes
+ * that path as C++ functions over its `param` class (no C ABI):
+ *   param::param_2des(string)            etoheom-cpu/lib/param.h:41, param.cpp:18-248
+ *   construct_ADO_set(param&)            etoheom-cpu/lib/utilize.h:18, utilize.cpp:26-36
+ *   construct_Hal(param&, H, rng)        etoheom-cpu/lib/dynamics.h:25, dynamics.cpp:3-51
+ *   polar_mat_set/_ranrot, compute_pulse_interaction   etoheom-cpu/lib/polar.h:26-30
+ *   twoD_spectrum_solver(param&, H, nv1, nv2, nv3, P)  etoheom-cpu/lib/dynamics.h:23,
+ *                                        dynamics.cpp:298-432 (GPU: HEOM_dynamics.h:36)
+ *   total_ADO_dynamics_Ht(param&, rho, drho, Ht)       etoheom-cpu/lib/dynamics.h:19
+ *   CPU_2DES / GPU_2DES main             etoheom-cpu/src/CPU_2DES.cpp:14-91,
+ *                                        etoheom-gpu/src/GPU_2DES.cu:25-88
+ * Each entry point below names the reference function it replaces.
+ *
+ * Conventions: every function returns HEOM_OK (0) or a negative HEOM_ERR_* code and
+ * never exits the process; heom_last_error() gives a thread-local message.  Complex
+ * numbers are interleaved (re, im) doubles; matrices are row-major N x N.  Output
+ * buffers are caller-owned host memory unless the name ends in _device.  A plan is
+ * bound to one CUDA device and stream and is not thread-safe; distinct plans may run
+ * concurrently.  There is no CPU fallback: without a usable CUDA device,
+ * heom_plan_create fails with HEOM_ERR_CUDA. */
+#ifndef HEOM_H
+#define HEOM_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HEOM_ABI_VERSION 1
+
+enum {
+  HEOM_OK = 0,
+  HEOM_ERR_ARG = -1,          /* bad argument / handle */
+  HEOM_ERR_IO = -2,           /* key file unreadable */
+  HEOM_ERR_PARSE = -3,        /* key file incomplete or inconsistent */
+  HEOM_ERR_CUDA = -4,         /* CUDA runtime failure or no device */
+  HEOM_ERR_NOMEM = -5,        /* host or device allocation failed */
+  HEOM_ERR_CAPACITY = -6,     /* output buffer too small / size above a limit */
+  HEOM_ERR_UNSUPPORTED = -7,  /* option not available for this problem */
+  HEOM_ERR_NUMERIC = -8,      /* non-finite value in the propagated state */
+  HEOM_ERR_TIMEOUT = -9       /* a bounded device-side wait expired */
+};
+
+/* Precision of the propagation. */
+enum {
+  HEOM_FP64_EXACT = 0, /* FP64, the reference's floating-point operation sequence:
+                          bit-identical P(t) to the reference CPU build */
+  HEOM_FP64 = 1,       /* FP64 everywhere, fused multiply-add, batched layout */
+  HEOM_FP32_BULK = 2   /* commutator and neighbour contractions in FP32 (FP32
+                          accumulation); state, RK4 accumulation, damping diagonal,
+                          site-energy diagonal and P(t) trace in FP64 */
+};
+
+/* Matrix selectors for heom_problem_get_matrix / heom_problem_set_matrix. */
+enum { HEOM_MAT_H = 0, HEOM_MAT_X0 = 1, HEOM_MAT_X1 = 2, HEOM_MAT_X2 = 3, HEOM_MAT_X3 = 4,
+       HEOM_MAT_HKEY = 5 };
+
+/* heom_problem_from_key flags. */
+enum { HEOM_KEY_SINGLE_MANIFOLD = 1 }; /* no two-exciton block (also: MANIFOLD single) */
+
+typedef struct heom_problem heom_problem;
+typedef struct heom_plan heom_plan;
+
+typedef struct {
+  int single_size, sys_size; /* SIZE and N = SIZE + (SIZE-1)(SIZE-2)/2 */
+  int K, K_m, L, n_ado;      /* sites, bath lines per site, depth, C(K*K_m+L, L) */
+  int n_sample;
+  unsigned long seed;
+  int n_steps;               /* RK4 steps of one trajectory (floor(nstep) + 1) */
+  int print_stride;          /* (int)(print_step / step_size) */
+  int n_record;              /* recorded P points of one trajectory */
+  float t_start, t_end, step_size, print_step;
+  double E0[3], tau[3], taup[3], w0[3]; /* pulses, E0 and w0 already divided by hbar */
+} heom_problem_info;
+
+/* Parse a key file with the reference CPU parser semantics (replaces
+ * param::param_2des, param.cpp:18-248, plus construct_ADO_set, utilize.cpp:26-36,
+ * and the RNG seeding of CPU_2DES.cpp:23-29). */
+int heom_problem_from_key(const char *path, int flags, heom_problem **out);
+int heom_problem_info_get(const heom_problem *p, heom_problem_info *info);
+/* Next disorder/orientation sample, drawing from the problem's RNG stream exactly as
+ * CPU_2DES.cpp:52-60 does: construct_Hal (dynamics.cpp:3-51), polar_mat_set,
+ * polar_mat_ranrot, compute_pulse_interaction (polar.cpp:17-101). */
+int heom_problem_prepare_sample(heom_problem *p);
+/* Same without random draws: zero disorder and no orientational rotation. */
+int heom_problem_prepare_identity(heom_problem *p);
+int heom_problem_reset_rng(heom_problem *p);
+int heom_problem_get_matrix(const heom_problem *p, int which, double *out);
+int heom_problem_set_matrix(heom_problem *p, int which, const double *in);
+/* ADO multi-indices, n_ado x (K*K_m) bytes, in the reference's order. */
+int heom_problem_get_ado(const heom_problem *p, unsigned char *out);
+void heom_problem_destroy(heom_problem *p);
+
+typedef struct {
+  int precision;    /* HEOM_FP64_EXACT / HEOM_FP64 / HEOM_FP32_BULK */
+  int device;       /* CUDA device ordinal */
+  void *stream;     /* cudaStream_t to run on; NULL = a stream owned by the plan */
+  int max_points;   /* capacity of one heom_run_scan call (0 = 1024) */
+  int autotune;     /* 1 = time candidate launch shapes at plan creation */
+} heom_opts;
+
+/* Device plan: uploads H, X[0..3], the ADO neighbour tables and the bath
+ * coefficients of the problem's current sample. */
+int heom_plan_create(const heom_problem *p, const heom_opts *opts, heom_plan **out);
+/* Re-upload H and X[0..3] after heom_problem_prepare_sample. */
+int heom_plan_update(heom_plan *plan, const heom_problem *p);
+
+/* One trajectory with pulse mask (nv1, nv2, nv3) (replaces twoD_spectrum_solver,
+ * dynamics.cpp:298-432; HEOM_dynamics.cu:489-658).  P receives the recorded
+ * Tr(rho_0 X[3]) points, *n_out their count. */
+int heom_run_traj(heom_plan *plan, int nv1, int nv2, int nv3, double *P, int cap, int *n_out);
+
+/* One 2DES point of the current sample: trajectories 111, 110, 101 and
+ * P = p111 - p110 - p101 (CPU_2DES.cpp:65-79).  p_traj (optional) receives the
+ * three trajectories, [3][cap] complex. */
+int heom_run_2des(heom_plan *plan, double *P, double *p_traj, int cap, int *n_out);
+
+/* A 2DES delay scan: n independent points (pulse times and end time replace the
+ * key file's), the whole scan in one persistent kernel launch replayed from a CUDA
+ * graph (replaces one CPU_2DES/GPU_2DES process per key file,
+ * script/cpu-script/submit_jobs.sh:49-67).  Output of point i: counts[i] combined
+ * P points at P + 2*offsets[i].  heom_scan_layout fills counts/offsets and returns
+ * the total number of complex points through *total. */
+typedef struct { double tau1, tau2, tau3; float t_end; int flags; } heom_scan_point;
+int heom_scan_layout(const heom_plan *plan, const heom_scan_point *pts, int n,
+                     long long *offsets, int *counts, long long *total);
+int heom_run_scan(heom_plan *plan, const heom_scan_point *pts, int n, double *P,
+                  const long long *offsets, const int *counts);
+/* Same with every buffer already in device memory; no host synchronisation. */
+int heom_run_scan_device(heom_plan *plan, const heom_scan_point *d_pts, int n, double *d_P,
+                         const long long *d_offsets);
+
+/* Launch shape chosen by the autotuner for this plan ("threads/CTA, CTAs/SM"). */
+int heom_plan_describe(const heom_plan *plan, char *buf, int len);
+/* Number of device kernel launches issued by this plan since creation. */
+long long heom_plan_launch_count(const heom_plan *plan);
+void heom_plan_destroy(heom_plan *plan);
+
+const char *heom_last_error(void);
+int heom_abi_version(void);
+
+/* Measured FP32 (fp64 = 0) or FP64 (fp64 = 1) FMA throughput of a device in TFLOP/s
+ * (2 flops per FMA) -- the roofline denominator for the propagation kernels, which run
+ * on the CUDA-core FMA pipes.  Measurement utility; no counterpart in the reference. */
+int heom_measure_fma_peak(int device, int fp64, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

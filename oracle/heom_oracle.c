@@ -1,0 +1,807 @@
+/* CPU oracle for the HEOM-ETO 2DES propagation path -- TEST INFRASTRUCTURE ONLY.
+ * See heom_oracle.h.  Each function cites the reference file:line it restates
+ * (paths relative to the reference project, etoheom-cpu/...). */
+#define _GNU_SOURCE
+#include "heom_oracle.h"
+
+#include <ctype.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* lib/constant.cpp:3-10 */
+static const double H_BAR = 5.308e3;
+static const double BOLTZ_K = 0.695;
+static const double PI_ = 3.141592653589793238462643383279502884L;
+
+typedef struct { double E0, tau0, taup, w0; } pulse_t;
+
+struct ho_problem {
+  int single_size, sys_size, K, K_m, L, n_sample, M, n_ado;
+  unsigned long seed;
+  int d_a[4096], d_b[4096]; /* d_map: level -> (a, b) for two-exciton levels */
+  double *Hkey, *Dis, *Xx, *Xy, *Xz, *X[4], *H; /* N x N complex */
+  double polar[3 * 4 * 2];                        /* 3 x 4 complex */
+  double angle[4];
+  int have_polar, have_dipole, have_bath, have_pulse;
+  double *alpha, *alpha_t, *gamma; /* K_m complex each (identical for every site) */
+  pulse_t pulses[3];
+  float t_start, t_end, step_size, print_step;
+  unsigned char *ado; /* n_ado x M */
+  int *up, *dn;       /* n_ado x M neighbour indices or -1 */
+  /* RNG (MT19937, restated as in oracle/gslshim) */
+  unsigned long mt[624];
+  int mti;
+};
+
+/* ---------------------------------------------------------------- complex */
+typedef struct { double r, i; } cplx;
+static inline cplx cx(double r, double i) { cplx z = {r, i}; return z; }
+static inline cplx cmul(cplx a, cplx b) { return cx(a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r); }
+static inline cplx cmul_real(cplx a, double x) { return cx(x * a.r, x * a.i); }
+static inline cplx cadd(cplx a, cplx b) { return cx(a.r + b.r, a.i + b.i); }
+static inline cplx cpolar(double r, double th) { return cx(r * cos(th), r * sin(th)); }
+static inline double cabs_(cplx a) { return hypot(a.r, a.i); }
+static const cplx C_ONE = {1.0, 0.0}, C_ZERO = {0.0, 0.0}, C_MINUS_ONE = {-1.0, 0.0};
+static const cplx C_I = {0.0, 1.0}, C_MINUS_I = {0.0, -1.0};
+
+#define EL(m, N, i, j) ((m) + 2 * ((size_t)(i) * (N) + (j)))
+static inline cplx get(const double *m, int N, int i, int j) { const double *p = EL(m, N, i, j); return cx(p[0], p[1]); }
+static inline void set(double *m, int N, int i, int j, cplx z) { double *p = EL(m, N, i, j); p[0] = z.r; p[1] = z.i; }
+
+/* C = alpha*A*B + beta*C with the reference-BLAS row-major loop order
+ * (the GSL zgemm the reference calls, dynamics.cpp:126-174).  Only the beta
+ * values 0 and 1 occur on this path. */
+static void zgemm(cplx alpha, const double *A, const double *B, cplx beta, double *C, int N) {
+  if (beta.r == 0.0 && beta.i == 0.0) {
+    for (int k = 0; k < 2 * N * N; k++) C[k] = 0.0;
+  } else if (!(beta.r == 1.0 && beta.i == 0.0)) {
+    for (int i = 0; i < N; i++)
+      for (int j = 0; j < N; j++) set(C, N, i, j, cmul(beta, get(C, N, i, j)));
+  }
+  if (alpha.r == 0.0 && alpha.i == 0.0) return;
+  for (int i = 0; i < N; i++)
+    for (int l = 0; l < N; l++) {
+      const double *a = EL(A, N, i, l);
+      const double tr = alpha.r * a[0] - alpha.i * a[1];
+      const double ti = alpha.r * a[1] + alpha.i * a[0];
+      if (tr == 0.0 && ti == 0.0) continue;
+      for (int j = 0; j < N; j++) {
+        const double *b = EL(B, N, l, j);
+        double *c = EL(C, N, i, j);
+        c[0] += tr * b[0] - ti * b[1];
+        c[1] += tr * b[1] + ti * b[0];
+      }
+    }
+}
+
+/* y += alpha*x over n complex entries (cblas_zaxpy, dynamics.cpp:139,389-417). */
+static void zaxpy(int n, cplx alpha, const double *x, double *y) {
+  if (fabs(alpha.r) == 0 && fabs(alpha.i) == 0) return;
+  for (int k = 0; k < n; k++) {
+    const double xr = x[2 * k], xi = x[2 * k + 1];
+    y[2 * k] += (alpha.r * xr - alpha.i * xi);
+    y[2 * k + 1] += (alpha.r * xi + alpha.i * xr);
+  }
+}
+
+/* gsl_matrix_complex_scale: a = a*x elementwise. */
+static void mscale(double *a, int n, cplx x) {
+  for (int k = 0; k < n; k++) {
+    const double ar = a[2 * k], ai = a[2 * k + 1];
+    a[2 * k] = ar * x.r - ai * x.i;
+    a[2 * k + 1] = ar * x.i + ai * x.r;
+  }
+}
+
+/* ---------------------------------------------------------------- RNG */
+static void rng_set(ho_problem *p, unsigned long s) {
+  if (s == 0) s = 4357;
+  p->mt[0] = s & 0xffffffffUL;
+  for (int i = 1; i < 624; i++)
+    p->mt[i] = (1812433253UL * (p->mt[i - 1] ^ (p->mt[i - 1] >> 30)) + (unsigned long)i) & 0xffffffffUL;
+  p->mti = 624;
+}
+static unsigned long rng_get(ho_problem *p) {
+  const unsigned long UP = 0x80000000UL, LO = 0x7fffffffUL;
+  if (p->mti >= 624) {
+    int k;
+    for (k = 0; k < 624; k++) {
+      unsigned long y = (p->mt[k] & UP) | (p->mt[(k + 1) % 624] & LO);
+      p->mt[k] = p->mt[(k + 397) % 624] ^ (y >> 1) ^ ((y & 1UL) ? 0x9908b0dfUL : 0UL);
+    }
+    p->mti = 0;
+  }
+  unsigned long k = p->mt[p->mti++];
+  k ^= (k >> 11);
+  k ^= (k << 7) & 0x9d2c5680UL;
+  k ^= (k << 15) & 0xefc60000UL;
+  k ^= (k >> 18);
+  return k & 0xffffffffUL;
+}
+static double rng_uniform(ho_problem *p) { return rng_get(p) / 4294967296.0; }
+static double rng_uniform_pos(ho_problem *p) { double x; do { x = rng_uniform(p); } while (x == 0); return x; }
+static double ran_gaussian(ho_problem *p, double sigma) {
+  double x, y, r2;
+  do {
+    x = -1 + 2 * rng_uniform_pos(p);
+    y = -1 + 2 * rng_uniform_pos(p);
+    r2 = x * x + y * y;
+  } while (r2 > 1.0 || r2 == 0);
+  return sigma * y * sqrt(-2.0 * log(r2) / r2);
+}
+static void ran_dir_3d(ho_problem *p, double *x, double *y, double *z) {
+  double s, a;
+  do {
+    *x = -1 + 2 * rng_uniform(p);
+    *y = -1 + 2 * rng_uniform(p);
+    s = (*x) * (*x) + (*y) * (*y);
+  } while (s > 1.0);
+  *z = -1 + 2 * s;
+  a = 2 * sqrt(1 - s);
+  *x *= a;
+  *y *= a;
+}
+
+/* ---------------------------------------------------------------- parser */
+static void seterr(char *err, int n, const char *fmt, ...) {
+  if (!err || n <= 0) return;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(err, (size_t)n, fmt, ap);
+  va_end(ap);
+}
+
+typedef struct { char *buf; size_t len, pos; int fail; } reader_t;
+/* std::getline semantics: returns 0 once the stream has failed (EOF with
+ * nothing extracted); the line is cleared on failure. */
+static int getline_(reader_t *r, char *line, size_t cap) {
+  line[0] = 0;
+  if (r->fail) return 0;
+  if (r->pos >= r->len) { r->fail = 1; return 0; }
+  size_t n = 0;
+  while (r->pos < r->len && r->buf[r->pos] != '\n') {
+    if (n + 1 < cap) line[n++] = r->buf[r->pos];
+    r->pos++;
+  }
+  if (r->pos < r->len) r->pos++;
+  line[n] = 0;
+  return 1;
+}
+
+/* istringstream >> T on successive whitespace tokens. */
+typedef struct { const char *s; int fail; } tok_t;
+static int next_tok(tok_t *t, char *out, size_t cap) {
+  if (t->fail) return 0;
+  while (*t->s && isspace((unsigned char)*t->s)) t->s++;
+  if (!*t->s) { t->fail = 1; return 0; }
+  size_t n = 0;
+  while (*t->s && !isspace((unsigned char)*t->s)) { if (n + 1 < cap) out[n++] = *t->s; t->s++; }
+  out[n] = 0;
+  return 1;
+}
+static int tok_double(tok_t *t, double *v) {
+  if (t->fail) return 0;
+  while (*t->s && isspace((unsigned char)*t->s)) t->s++;
+  char *end;
+  double x = strtod(t->s, &end);
+  if (end == t->s) { t->fail = 1; return 0; }
+  t->s = end; *v = x; return 1;
+}
+static int tok_float(tok_t *t, float *v) {
+  if (t->fail) return 0;
+  while (*t->s && isspace((unsigned char)*t->s)) t->s++;
+  char *end;
+  float x = strtof(t->s, &end);
+  if (end == t->s) { t->fail = 1; return 0; }
+  t->s = end; *v = x; return 1;
+}
+static int tok_long(tok_t *t, long *v) {
+  if (t->fail) return 0;
+  while (*t->s && isspace((unsigned char)*t->s)) t->s++;
+  char *end;
+  long x = strtol(t->s, &end, 10);
+  if (end == t->s) { t->fail = 1; return 0; }
+  t->s = end; *v = x; return 1;
+}
+static int tok_ulong(tok_t *t, unsigned long *v) {
+  if (t->fail) return 0;
+  while (*t->s && isspace((unsigned char)*t->s)) t->s++;
+  char *end;
+  unsigned long x = strtoul(t->s, &end, 10);
+  if (end == t->s) { t->fail = 1; return 0; }
+  t->s = end; *v = x; return 1;
+}
+
+static double *zmat(int N) { return (double *)calloc((size_t)2 * N * N + 2, sizeof(double)); }
+
+/* ADO enumeration (utilize.cpp:3-36): all M-digit strings with digits 0..L and
+ * digit sum <= L, in the recursion's (lexicographic) order. */
+static void build_ado_rec(ho_problem *p, unsigned char *cur, int depth, int sum, int *count, int store) {
+  if (depth == p->M) {
+    if (sum <= p->L) {
+      if (store) memcpy(p->ado + (size_t)(*count) * p->M, cur, (size_t)p->M);
+      (*count)++;
+    }
+    return;
+  }
+  for (int c = 0; c <= p->L; c++)
+    if (sum + c <= p->L) {
+      cur[depth] = (unsigned char)c;
+      build_ado_rec(p, cur, depth + 1, sum + c, count, store);
+    }
+}
+static int find_ado(const ho_problem *p, const unsigned char *key) {
+  int lo = 0, hi = p->n_ado - 1;
+  while (lo <= hi) {
+    int mid = (lo + hi) / 2;
+    int c = memcmp(p->ado + (size_t)mid * p->M, key, (size_t)p->M);
+    if (c == 0) return mid;
+    if (c < 0) lo = mid + 1; else hi = mid - 1;
+  }
+  return -1;
+}
+static void build_ado(ho_problem *p) {
+  unsigned char cur[256];
+  int count = 0;
+  build_ado_rec(p, cur, 0, 0, &count, 0);
+  p->n_ado = count;
+  p->ado = (unsigned char *)malloc((size_t)count * p->M + 1);
+  count = 0;
+  build_ado_rec(p, cur, 0, 0, &count, 1);
+  p->up = (int *)malloc(sizeof(int) * (size_t)count * p->M + 4);
+  p->dn = (int *)malloc(sizeof(int) * (size_t)count * p->M + 4);
+  unsigned char key[256];
+  for (int n = 0; n < count; n++)
+    for (int o = 0; o < p->M; o++) {
+      memcpy(key, p->ado + (size_t)n * p->M, (size_t)p->M);
+      key[o] = (unsigned char)(key[o] + 1);
+      p->up[n * p->M + o] = find_ado(p, key);
+      key[o] = (unsigned char)(key[o] - 2);
+      p->dn[n * p->M + o] = (p->ado[(size_t)n * p->M + o] > 0) ? find_ado(p, key) : -1;
+    }
+}
+
+int ho_load_key(const char *path, int single_manifold, ho_problem **out, char *err, int errlen) {
+  FILE *f = fopen(path, "rb");
+  if (!f) { seterr(err, errlen, "cannot open key file '%s'", path); return -1; }
+  fseek(f, 0, SEEK_END);
+  long len = ftell(f);
+  fseek(f, 0, SEEK_SET);
+  reader_t rd = {0};
+  rd.buf = (char *)malloc((size_t)len + 1);
+  rd.len = fread(rd.buf, 1, (size_t)len, f);
+  fclose(f);
+  ho_problem *p = (ho_problem *)calloc(1, sizeof *p);
+  static char line[1 << 16];
+  char kw[256] = "", tokbuf[256];
+  int K_m_lines = 0;
+  /* param.cpp:102-332: keyword loop; the keyword persists over lines that hold
+   * no token, exactly like `iss >> key_word` on a whitespace-only line. */
+  while (getline_(&rd, line, sizeof line)) {
+    if (line[0] == 0 || line[0] == '#') continue;
+    tok_t t = {line, 0};
+    if (next_tok(&t, tokbuf, sizeof tokbuf)) snprintf(kw, sizeof kw, "%s", tokbuf);
+    if (!strcmp(kw, "HEOM")) {
+      getline_(&rd, line, sizeof line);
+      tok_t v = {line, 0};
+      long a = p->K, b = p->L;
+      if (tok_long(&v, &a)) { p->K = (int)a; if (tok_long(&v, &b)) p->L = (int)b; }
+    } else if (!strcmp(kw, "SIZE")) {
+      getline_(&rd, line, sizeof line);
+      tok_t v = {line, 0};
+      long s = p->single_size;
+      if (tok_long(&v, &s)) p->single_size = (int)s;
+      int ss = p->single_size;
+      p->sys_size = single_manifold ? ss : ss + (ss - 1) * (ss - 2) / 2;
+      if (!single_manifold) {
+        int ct = ss;
+        for (int i = 1; i < ss; i++)
+          for (int j = i; j < ss; j++)
+            if (i != j && ct < 4096) { p->d_a[ct] = i; p->d_b[ct] = j; ct++; }
+      }
+    } else if (!strcmp(kw, "DISORDER")) {
+      getline_(&rd, line, sizeof line);
+      tok_t v = {line, 0};
+      long ns = p->n_sample;
+      unsigned long sd = p->seed;
+      if (tok_long(&v, &ns)) { p->n_sample = (int)ns; if (tok_ulong(&v, &sd)) p->seed = sd; }
+      int N = p->sys_size;
+      free(p->Dis);
+      p->Dis = zmat(N);
+      for (int i = 0; i < N; i++) {
+        getline_(&rd, line, sizeof line);
+        tok_t r = {line, 0};
+        double x;
+        for (int j = 0; tok_double(&r, &x); j++)
+          if (j < N) set(p->Dis, N, i, j, cx(x / H_BAR, 0.0));
+      }
+    } else if (!strcmp(kw, "HAMILTONIAN")) {
+      int N = p->sys_size;
+      free(p->Hkey);
+      p->Hkey = zmat(N);
+      for (int i = 0; i < p->single_size; i++) {
+        getline_(&rd, line, sizeof line);
+        tok_t r = {line, 0};
+        double x;
+        for (int j = 0; tok_double(&r, &x); j++)
+          if (j < N && i < N) set(p->Hkey, N, i, j, cx(x / H_BAR, 0.0));
+      }
+    } else if (!strcmp(kw, "DIPOLE")) {
+      getline_(&rd, line, sizeof line);
+      tok_t v = {line, 0};
+      long nd = 0;
+      tok_long(&v, &nd);
+      int N = p->sys_size;
+      free(p->Xx); free(p->Xy); free(p->Xz);
+      p->Xx = zmat(N); p->Xy = zmat(N); p->Xz = zmat(N);
+      for (long k = 0; k < nd; k++) {
+        getline_(&rd, line, sizeof line);
+        tok_t r = {line, 0};
+        long i = 0, j = 0;
+        double x = 0, y = 0, z = 0;
+        if (tok_long(&r, &i) && tok_long(&r, &j) && tok_double(&r, &x) && tok_double(&r, &y)) tok_double(&r, &z);
+        if (i >= 0 && i < N && j >= 0 && j < N) {
+          set(p->Xx, N, (int)i, (int)j, cx(x, 0.0));
+          set(p->Xy, N, (int)i, (int)j, cx(y, 0.0));
+          set(p->Xz, N, (int)i, (int)j, cx(z, 0.0));
+        }
+      }
+      /* two-exciton columns, param.cpp:200-230 */
+      double *XS[3] = {p->Xx, p->Xy, p->Xz};
+      for (int q = 0; q < 3; q++)
+        for (int i = 0; i < N; i++)
+          for (int j = p->single_size; j < N; j++) {
+            int a = p->d_a[j], b = p->d_b[j];
+            double x1 = get(XS[q], N, 0, a).r, x2 = get(XS[q], N, 0, b).r;
+            double x = (b == i ? 1.0 : 0.0) * x1 + (a == i ? 1.0 : 0.0) * x2;
+            set(XS[q], N, i, j, cx(x, 0.0));
+          }
+      p->have_dipole = 1;
+    } else if (!strcmp(kw, "POLARIZATION")) {
+      getline_(&rd, line, sizeof line);
+      tok_t v = {line, 0};
+      double ang[4] = {0, 0, 0, 0};
+      for (int q = 0; q < 4; q++) if (!tok_double(&v, &ang[q])) break;
+      for (int q = 0; q < 4; q++) p->angle[q] = ang[q] * PI_ / 180;
+      int N = p->sys_size;
+      for (int q = 0; q < 4; q++) { free(p->X[q]); p->X[q] = zmat(N); }
+      p->have_polar = 1;
+    } else if (!strcmp(kw, "TEMPERATURE")) {
+      getline_(&rd, line, sizeof line); /* beta is unused on the 2DES path */
+    } else if (!strcmp(kw, "BATH")) {
+      getline_(&rd, line, sizeof line);
+      tok_t v = {line, 0};
+      double l = 0;
+      tok_double(&v, &l);
+      if (!p->Hkey) { seterr(err, errlen, "BATH before HAMILTONIAN"); goto fail; }
+      int N = p->sys_size;
+      for (int i = 0; i < p->K; i++) {
+        int q = i + 1; /* param.cpp:189: lambda shifts the single-excitation levels */
+        if (q < N) set(p->Hkey, N, q, q, cx(get(p->Hkey, N, q, q).r + l, 0.0));
+      }
+      getline_(&rd, line, sizeof line);
+      tok_t v2 = {line, 0};
+      long nm = 0;
+      tok_long(&v2, &nm);
+      free(p->alpha); free(p->alpha_t); free(p->gamma);
+      p->alpha = (double *)calloc(2 * (size_t)(nm > 0 ? nm : 1), sizeof(double));
+      p->alpha_t = (double *)calloc(2 * (size_t)(nm > 0 ? nm : 1), sizeof(double));
+      p->gamma = (double *)calloc(2 * (size_t)(nm > 0 ? nm : 1), sizeof(double));
+      for (long k = 0; k < nm; k++) {
+        getline_(&rd, line, sizeof line);
+        tok_t r = {line, 0};
+        double a = 0, b = 0, g = 0, w = 0;
+        if (tok_double(&r, &a) && tok_double(&r, &b) && tok_double(&r, &g)) tok_double(&r, &w);
+        p->alpha[2 * k] = a; p->alpha[2 * k + 1] = b;
+        p->alpha_t[2 * k] = a; p->alpha_t[2 * k + 1] = -b;
+        p->gamma[2 * k] = g; p->gamma[2 * k + 1] = w;
+      }
+      K_m_lines = (int)nm;
+      p->K_m = K_m_lines;
+      p->have_bath = 1;
+    } else if (!strcmp(kw, "PULSE")) {
+      getline_(&rd, line, sizeof line);
+      tok_t v = {line, 0};
+      long n = 0;
+      tok_long(&v, &n);
+      if (n != 3) { seterr(err, errlen, "Only support 3 pulses simulation."); goto fail; }
+      for (int i = 0; i < 3; i++) {
+        getline_(&rd, line, sizeof line);
+        tok_t r = {line, 0};
+        pulse_t *q = &p->pulses[i];
+        if (tok_double(&r, &q->E0) && tok_double(&r, &q->tau0) && tok_double(&r, &q->taup)) tok_double(&r, &q->w0);
+        q->w0 = q->w0 / H_BAR;
+        q->E0 = q->E0 / H_BAR;
+      }
+      p->have_pulse = 1;
+    } else if (!strcmp(kw, "TIME")) {
+      getline_(&rd, line, sizeof line);
+      tok_t v = {line, 0};
+      if (tok_float(&v, &p->t_start) && tok_float(&v, &p->t_end) && tok_float(&v, &p->step_size))
+        tok_float(&v, &p->print_step);
+    }
+  }
+  free(rd.buf);
+  rd.buf = NULL;
+  if (p->sys_size <= 0 || !p->Hkey) { seterr(err, errlen, "key file lacks SIZE/HAMILTONIAN"); goto fail; }
+  if (!p->have_bath || p->K_m <= 0) { seterr(err, errlen, "key file lacks a BATH block"); goto fail; }
+  if (!p->Dis || p->n_sample <= 0) { seterr(err, errlen, "key file lacks a DISORDER block with n_sample > 0"); goto fail; }
+  if (!p->have_polar) { seterr(err, errlen, "key file lacks POLARIZATION"); goto fail; }
+  if (!p->have_dipole) { seterr(err, errlen, "key file lacks DIPOLE"); goto fail; }
+  if (!p->have_pulse) { seterr(err, errlen, "key file lacks PULSE"); goto fail; }
+  if (p->step_size <= 0 || (int)(p->print_step / p->step_size) <= 0) { seterr(err, errlen, "TIME step/print step invalid"); goto fail; }
+  p->M = p->K * p->K_m;
+  if (p->M <= 0 || p->M > 255 || p->L < 0 || p->L > 255) { seterr(err, errlen, "HEOM K*K_m / L out of range"); goto fail; }
+  build_ado(p);
+  p->H = zmat(p->sys_size);
+  rng_set(p, p->seed);
+  *out = p;
+  return 0;
+fail:
+  free(rd.buf);
+  ho_free(p);
+  return -1;
+}
+
+void ho_free(ho_problem *p) {
+  if (!p) return;
+  free(p->Hkey); free(p->Dis); free(p->Xx); free(p->Xy); free(p->Xz); free(p->H);
+  for (int q = 0; q < 4; q++) free(p->X[q]);
+  free(p->alpha); free(p->alpha_t); free(p->gamma);
+  free(p->ado); free(p->up); free(p->dn);
+  free(p);
+}
+
+static int n_steps_of(const ho_problem *p) {
+  float nstep = (p->t_end - p->t_start) / p->step_size;
+  int n = 0;
+  for (int i = 0; i <= nstep; i++) n++;
+  return n;
+}
+
+void ho_info(const ho_problem *p, int *info) {
+  info[0] = p->single_size; info[1] = p->sys_size; info[2] = p->K; info[3] = p->K_m; info[4] = p->L;
+  info[5] = p->n_ado; info[6] = p->n_sample; info[7] = n_steps_of(p);
+  info[8] = (int)(p->print_step / p->step_size); info[9] = (int)(p->seed & 0x7fffffff);
+}
+
+void ho_rng_reset(ho_problem *p) { rng_set(p, p->seed); }
+
+/* construct_Hal (dynamics.cpp:3-51): disorder draws, diagonal sort, two-exciton block. */
+static void construct_hal(ho_problem *p, int draw) {
+  int N = p->sys_size, s = p->single_size;
+  double *dH = zmat(N);
+  for (int i = 0; i < s; i++)
+    for (int j = 0; j < s; j++) {
+      double sigma = get(p->Dis, N, i, j).r, tmp;
+      if (fabs(sigma) < 1e-10 || !draw) tmp = 0;
+      else tmp = ran_gaussian(p, sigma);
+      set(dH, N, i, j, cx(tmp, 0.0));
+    }
+  memcpy(p->H, p->Hkey, sizeof(double) * 2 * (size_t)N * N);
+  for (int k = 0; k < 2 * N * N; k++) p->H[k] += dH[k];
+  free(dH);
+  double *Ht = (double *)calloc((size_t)s + 1, sizeof(double));
+  for (int i = 1; i < s; i++) Ht[i] = get(p->H, N, i, i).r;
+  /* std::sort of all single_size entries, index 0 (= 0.0) included */
+  for (int i = 1; i < s; i++) {
+    double v = Ht[i];
+    int j = i - 1;
+    while (j >= 0 && Ht[j] > v) { Ht[j + 1] = Ht[j]; j--; }
+    Ht[j + 1] = v;
+  }
+  for (int i = 1; i < s; i++) set(p->H, N, i, i, cx(Ht[i], 0.0));
+  free(Ht);
+  if (p->sys_size == p->single_size) return; /* single-manifold extension */
+  for (int i = s; i < N; i++)
+    for (int j = s; j < N; j++) {
+      int a = p->d_a[i], b = p->d_b[i];
+      if (i == j) {
+        set(p->H, N, i, i, cadd(get(p->H, N, a, a), get(p->H, N, b, b)));
+      } else {
+        int c = p->d_a[j], d = p->d_b[j];
+        double x1 = (double)(a == c) * (1 - (double)(b == d)) * get(p->H, N, b, d).r;
+        double x2 = (double)(a == d) * (1 - (double)(b == c)) * get(p->H, N, b, c).r;
+        double x3 = (double)(b == c) * (1 - (double)(a == d)) * get(p->H, N, a, d).r;
+        double x4 = (double)(b == d) * (1 - (double)(a == c)) * get(p->H, N, a, c).r;
+        set(p->H, N, i, j, cx(x1 + x2 + x3 + x4, 0.0));
+      }
+    }
+}
+
+static void vnorm(double *v) {
+  double a = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  v[0] = v[0] / a; v[1] = v[1] / a; v[2] = v[2] / a;
+}
+
+/* polar_mat_set / polar_mat_ranrot / compute_pulse_interaction (polar.cpp:17-101). */
+static void orient(ho_problem *p, int rotate) {
+  double *pol = p->polar;
+  for (int i = 0; i < 4; i++) {
+    pol[2 * (0 * 4 + i)] = 0.0; pol[2 * (0 * 4 + i) + 1] = 0.0;
+    pol[2 * (1 * 4 + i)] = sin(p->angle[i]); pol[2 * (1 * 4 + i) + 1] = 0.0;
+    pol[2 * (2 * 4 + i)] = cos(p->angle[i]); pol[2 * (2 * 4 + i) + 1] = 0.0;
+  }
+  if (rotate) {
+    double a[3] = {0}, b[3] = {0}, c[3] = {0};
+    ran_dir_3d(p, c, c + 1, c + 2);
+    vnorm(c);
+    ran_dir_3d(p, a, a + 1, a + 2);
+    double prod = a[0] * c[0] + a[1] * c[1] + a[2] * c[2];
+    a[0] = a[0] - prod * c[0]; a[1] = a[1] - prod * c[1]; a[2] = a[2] - prod * c[2];
+    vnorm(a);
+    b[0] = c[1] * a[2] - c[2] * a[1];
+    b[1] = c[2] * a[0] - c[0] * a[2];
+    b[2] = c[0] * a[1] - c[1] * a[0];
+    double R[3][3][2] = {{{0}}};
+    for (int i = 0; i < 3; i++) { R[0][i][0] = a[i]; R[1][i][0] = b[i]; R[2][i][0] = c[i]; }
+    double tmp[3][4][2];
+    /* zgemm(ONE, rotmat (3x3), polar (3x4), ZERO, tmp) */
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 4; j++) tmp[i][j][0] = tmp[i][j][1] = 0.0;
+    for (int i = 0; i < 3; i++)
+      for (int l = 0; l < 3; l++) {
+        const double tr = C_ONE.r * R[i][l][0] - C_ONE.i * R[i][l][1];
+        const double ti = C_ONE.r * R[i][l][1] + C_ONE.i * R[i][l][0];
+        if (tr == 0.0 && ti == 0.0) continue;
+        for (int j = 0; j < 4; j++) {
+          const double *bb = &pol[2 * (l * 4 + j)];
+          tmp[i][j][0] += tr * bb[0] - ti * bb[1];
+          tmp[i][j][1] += tr * bb[1] + ti * bb[0];
+        }
+      }
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 4; j++) { pol[2 * (i * 4 + j)] = tmp[i][j][0]; pol[2 * (i * 4 + j) + 1] = tmp[i][j][1]; }
+  }
+  int N = p->sys_size, nn = N * N;
+  const double *XS[3] = {p->Xx, p->Xy, p->Xz};
+  double *mt = zmat(N);
+  for (int i = 0; i < 4; i++) {
+    memset(p->X[i], 0, sizeof(double) * 2 * (size_t)nn);
+    for (int j = 0; j < 3; j++) {
+      cplx E = cx(pol[2 * (j * 4 + i)], pol[2 * (j * 4 + i) + 1]);
+      memcpy(mt, XS[j], sizeof(double) * 2 * (size_t)nn);
+      mscale(mt, nn, E);
+      for (int k = 0; k < 2 * nn; k++) p->X[i][k] += mt[k];
+    }
+  }
+  free(mt);
+}
+
+void ho_prepare_sample(ho_problem *p) { construct_hal(p, 1); orient(p, 1); }
+void ho_prepare_identity(ho_problem *p) { construct_hal(p, 0); orient(p, 0); }
+
+int ho_get_matrix(const ho_problem *p, int which, double *out) {
+  const double *m = which == HO_H ? p->H : which == HO_HKEY ? p->Hkey : (which >= 1 && which <= 4) ? p->X[which - 1] : NULL;
+  if (!m) return -1;
+  memcpy(out, m, sizeof(double) * 2 * (size_t)p->sys_size * p->sys_size);
+  return 0;
+}
+int ho_set_matrix(ho_problem *p, int which, const double *in) {
+  double *m = which == HO_H ? p->H : which == HO_HKEY ? p->Hkey : (which >= 1 && which <= 4) ? p->X[which - 1] : NULL;
+  if (!m) return -1;
+  memcpy(m, in, sizeof(double) * 2 * (size_t)p->sys_size * p->sys_size);
+  return 0;
+}
+void ho_get_ado(const ho_problem *p, unsigned char *out) { memcpy(out, p->ado, (size_t)p->n_ado * p->M); }
+void ho_get_bath(const ho_problem *p, double *out) {
+  for (int k = 0; k < p->K_m; k++) {
+    out[4 * k] = p->alpha[2 * k]; out[4 * k + 1] = p->alpha[2 * k + 1];
+    out[4 * k + 2] = p->gamma[2 * k]; out[4 * k + 3] = p->gamma[2 * k + 1];
+  }
+}
+
+/* ---------------------------------------------------------------- RHS */
+/* total_ADO_dynamics_Ht (dynamics.cpp:117-179).
+ * HO_DENSE multiplies by the one-hot S_j with full zgemm calls, exactly as the
+ * reference; HO_STRUCTURED touches only row/column s = j+1 and performs the
+ * same floating-point operations on every element that the dense form
+ * changes, so the two agree bit for bit. */
+void ho_rhs(ho_problem *p, const double *V, const double *rho, double *drho, int mode) {
+  const int N = p->sys_size, nn = N * N, K = p->K, Km = p->K_m, M = p->M;
+  double *S = NULL;
+  if (mode == HO_DENSE) S = zmat(N);
+  for (int i = 0; i < p->n_ado; i++) {
+    const double *r_i = rho + 2 * (size_t)i * nn;
+    double *d_i = drho + 2 * (size_t)i * nn;
+    const unsigned char *n_i = p->ado + (size_t)i * M;
+    zgemm(C_I, r_i, V, C_ZERO, d_i, N);
+    zgemm(C_MINUS_I, V, r_i, C_ONE, d_i, N);
+    if (i != 0) {
+      cplx x = C_ZERO;
+      for (int j = 0; j < K; j++)
+        for (int k = 0; k < Km; k++) {
+          int off = j + k * K;
+          if ((int)n_i[off] == 0) continue;
+          cplx y = cmul(C_MINUS_ONE, cmul_real(cx(p->gamma[2 * k], p->gamma[2 * k + 1]), (int)n_i[off]));
+          x = cadd(x, y);
+        }
+      zaxpy(nn, x, r_i, d_i);
+    }
+    for (int j = 0; j < K; j++)
+      for (int k = 0; k < Km; k++) {
+        int off = j + k * K;
+        if ((int)n_i[off] >= p->L) continue;
+        int t = p->up[i * M + off];
+        if (t < 0) continue;
+        const double *r_t = rho + 2 * (size_t)t * nn;
+        double x = sqrt(((double)n_i[off] + 1) * cabs_(cx(p->alpha[2 * k], p->alpha[2 * k + 1])));
+        int s = j + 1; /* S_j = |j+1><j+1| (param.cpp:190-195) */
+        cplx a1 = cmul_real(C_MINUS_I, x), a2 = cmul_real(C_I, x);
+        if (mode == HO_DENSE) {
+          memset(S, 0, sizeof(double) * 2 * (size_t)nn);
+          set(S, N, s, s, C_ONE);
+          zgemm(a1, r_t, S, C_ONE, d_i, N);
+          zgemm(a2, S, r_t, C_ONE, d_i, N);
+        } else {
+          for (int r = 0; r < N; r++) { /* rho+ S_j: column s, temp = a1*rho+[r][s] times S[s][s] = 1 */
+            const double *z = EL(r_t, N, r, s);
+            const double tr = a1.r * z[0] - a1.i * z[1], ti = a1.r * z[1] + a1.i * z[0];
+            if (tr == 0.0 && ti == 0.0) continue;
+            double *c = EL(d_i, N, r, s);
+            c[0] += tr * 1.0 - ti * 0.0;
+            c[1] += tr * 0.0 + ti * 1.0;
+          }
+          { /* S_j rho+: row s, temp = a2*S[s][s] */
+            const double tr = a2.r * 1.0 - a2.i * 0.0, ti = a2.r * 0.0 + a2.i * 1.0;
+            if (!(tr == 0.0 && ti == 0.0))
+              for (int c2 = 0; c2 < N; c2++) {
+                const double *z = EL(r_t, N, s, c2);
+                double *c = EL(d_i, N, s, c2);
+                c[0] += tr * z[0] - ti * z[1];
+                c[1] += tr * z[1] + ti * z[0];
+              }
+          }
+        }
+      }
+    if (i != 0) {
+      for (int j = 0; j < K; j++)
+        for (int k = 0; k < Km; k++) {
+          int off = j + k * K;
+          if ((int)n_i[off] <= 0) continue;
+          int t = p->dn[i * M + off];
+          if (t < 0) continue;
+          const double *r_t = rho + 2 * (size_t)t * nn;
+          cplx al = cx(p->alpha[2 * k], p->alpha[2 * k + 1]), alt = cx(p->alpha_t[2 * k], p->alpha_t[2 * k + 1]);
+          double y = sqrt((double)n_i[off] / cabs_(al));
+          cplx x1 = cmul(C_I, cmul_real(al, y));
+          cplx x2 = cmul(C_MINUS_I, cmul_real(alt, y));
+          int s = j + 1; /* S_j = |j+1><j+1| (param.cpp:190-195) */
+          if (mode == HO_DENSE) {
+            memset(S, 0, sizeof(double) * 2 * (size_t)nn);
+            set(S, N, s, s, C_ONE);
+            zgemm(x1, S, r_t, C_ONE, d_i, N);
+            zgemm(x2, r_t, S, C_ONE, d_i, N);
+          } else {
+            { /* S_j rho-: row s */
+              const double tr = x1.r * 1.0 - x1.i * 0.0, ti = x1.r * 0.0 + x1.i * 1.0;
+              if (!(tr == 0.0 && ti == 0.0))
+                for (int c2 = 0; c2 < N; c2++) {
+                  const double *z = EL(r_t, N, s, c2);
+                  double *c = EL(d_i, N, s, c2);
+                  c[0] += tr * z[0] - ti * z[1];
+                  c[1] += tr * z[1] + ti * z[0];
+                }
+            }
+            for (int r = 0; r < N; r++) { /* rho- S_j: column s */
+              const double *z = EL(r_t, N, r, s);
+              const double tr = x2.r * z[0] - x2.i * z[1], ti = x2.r * z[1] + x2.i * z[0];
+              if (tr == 0.0 && ti == 0.0) continue;
+              double *c = EL(d_i, N, r, s);
+              c[0] += tr * 1.0 - ti * 0.0;
+              c[1] += tr * 0.0 + ti * 1.0;
+            }
+          }
+        }
+    }
+  }
+  free(S);
+}
+
+/* ---------------------------------------------------------------- solver */
+/* build_V_matrix / build_V_dagger_matrix (TD_hamiltonian.cpp:5-31). */
+static cplx field(const pulse_t *q, float t, int dagger) {
+  double E = q->E0 * exp(-2.77 * (t - q->tau0) * (t - q->tau0) / q->taup / q->taup);
+  return dagger ? cpolar(E, -q->w0 * (t - q->tau0)) : cpolar(E, q->w0 * (t - q->tau0));
+}
+
+/* twoD_spectrum_solver (dynamics.cpp:298-419). */
+int ho_traj(ho_problem *p, int nv1, int nv2, int nv3, int mode, int max_steps, double *P, int cap, int *npts) {
+  const int N = p->sys_size, nn = N * N, na = p->n_ado;
+  const size_t tot = (size_t)na * nn;
+  double *rho = (double *)calloc(2 * tot, sizeof(double));
+  double *k1 = (double *)calloc(2 * tot, sizeof(double)), *k2 = (double *)calloc(2 * tot, sizeof(double));
+  double *k3 = (double *)calloc(2 * tot, sizeof(double)), *k4 = (double *)calloc(2 * tot, sizeof(double));
+  double *V = zmat(N), *Vp = zmat(N), *Pm = zmat(N), *Xt2 = zmat(N), *Xt3 = zmat(N);
+  if (!rho || !k1 || !k2 || !k3 || !k4) return -1;
+  rho[0] = 1.0; /* reset_rho, param.cpp:350-353 */
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < N; j++) { set(Xt2, N, i, j, get(p->X[1], N, j, i)); set(Xt3, N, i, j, get(p->X[2], N, j, i)); }
+  const double b[4] = {1.0 / 6, 2.0 / 6, 2.0 / 6, 1.0 / 6};
+  float nstep = (p->t_end - p->t_start) / p->step_size;
+  float t = p->t_start;
+  int print_step = (int)(p->print_step / p->step_size);
+  int n = 0;
+  for (int i = 0; i <= nstep; i++) {
+    if (max_steps > 0 && i >= max_steps) break;
+    memcpy(V, p->H, sizeof(double) * 2 * (size_t)nn);
+    const int nv[3] = {nv1, nv2, nv3};
+    const double *Xs[3] = {p->X[0], Xt2, Xt3};
+    for (int q = 0; q < 3; q++) {
+      if (nv[q] == 1 && fabs(t - p->pulses[q].tau0) <= p->pulses[q].taup * 2) {
+        cplx e = field(&p->pulses[q], t, q > 0);
+        memcpy(Vp, Xs[q], sizeof(double) * 2 * (size_t)nn);
+        mscale(Vp, nn, e);
+        for (int k = 0; k < 2 * nn; k++) V[k] -= Vp[k];
+      }
+    }
+    if (t >= p->pulses[2].tau0 && i % print_step == 0) {
+      zgemm(C_ONE, rho, p->X[3], C_ZERO, Pm, N);
+      cplx tr = C_ZERO;
+      for (int j = 0; j < N; j++) tr = cadd(tr, get(Pm, N, j, j));
+      if (n < cap) { P[2 * n] = tr.r; P[2 * n + 1] = tr.i; }
+      n++;
+    }
+    cplx x;
+    ho_rhs(p, V, rho, k1, mode);
+    x = cx(p->step_size * 0.5, 0.0);
+    zaxpy((int)tot, x, k1, rho);
+    ho_rhs(p, V, rho, k2, mode);
+    x = cmul_real(x, -1);
+    zaxpy((int)tot, x, k1, rho);
+    x = cx(p->step_size * 0.5, 0.0);
+    zaxpy((int)tot, x, k2, rho);
+    ho_rhs(p, V, rho, k3, mode);
+    x = cmul_real(x, -1);
+    zaxpy((int)tot, x, k2, rho);
+    x = cx(p->step_size, 0.0);
+    zaxpy((int)tot, x, k3, rho);
+    ho_rhs(p, V, rho, k4, mode);
+    x = cmul_real(x, -1);
+    zaxpy((int)tot, x, k3, rho);
+    x = cx(p->step_size * b[0], 0.0); zaxpy((int)tot, x, k1, rho);
+    x = cx(p->step_size * b[1], 0.0); zaxpy((int)tot, x, k2, rho);
+    x = cx(p->step_size * b[2], 0.0); zaxpy((int)tot, x, k3, rho);
+    x = cx(p->step_size * b[3], 0.0); zaxpy((int)tot, x, k4, rho);
+    t += p->step_size;
+  }
+  *npts = n;
+  free(rho); free(k1); free(k2); free(k3); free(k4);
+  free(V); free(Vp); free(Pm); free(Xt2); free(Xt3);
+  return 0;
+}
+
+/* CPU_2DES main (CPU_2DES.cpp:14-91). */
+int ho_2des(ho_problem *p, int mode, int max_steps, double *P, int cap, int *npts, double *traj) {
+  rng_set(p, p->seed);
+  double *p1 = (double *)calloc(2 * (size_t)cap + 2, sizeof(double));
+  double *p2 = (double *)calloc(2 * (size_t)cap + 2, sizeof(double));
+  double *p3 = (double *)calloc(2 * (size_t)cap + 2, sizeof(double));
+  double *acc = (double *)calloc(2 * (size_t)cap + 2, sizeof(double));
+  int n1 = 0, n2 = 0, n3 = 0;
+  for (int s = 0; s < p->n_sample; s++) {
+    ho_prepare_sample(p);
+    if (ho_traj(p, 1, 1, 1, mode, max_steps, p1, cap, &n1) || ho_traj(p, 1, 1, 0, mode, max_steps, p2, cap, &n2) ||
+        ho_traj(p, 1, 0, 1, mode, max_steps, p3, cap, &n3))
+      return -1;
+    int m = n1 < cap ? n1 : cap;
+    for (int j = 0; j < m; j++) {
+      double re = p1[2 * j] - p2[2 * j] - p3[2 * j];
+      double im = p1[2 * j + 1] - p2[2 * j + 1] - p3[2 * j + 1];
+      acc[2 * j] += re / p->n_sample;
+      acc[2 * j + 1] += im / p->n_sample;
+      if (traj) {
+        double *tp = traj + 2 * (size_t)cap * 3 * s;
+        tp[2 * j] = p1[2 * j]; tp[2 * j + 1] = p1[2 * j + 1];
+        tp[2 * (cap + j)] = p2[2 * j]; tp[2 * (cap + j) + 1] = p2[2 * j + 1];
+        tp[2 * (2 * cap + j)] = p3[2 * j]; tp[2 * (2 * cap + j) + 1] = p3[2 * j + 1];
+      }
+    }
+  }
+  *npts = n1;
+  memcpy(P, acc, sizeof(double) * 2 * (size_t)(n1 < cap ? n1 : cap));
+  free(p1); free(p2); free(p3); free(acc);
+  return 0;
+}

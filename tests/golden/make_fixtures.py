@@ -1,0 +1,235 @@
+"""Generate the test fixtures: key files and golden P(t) vectors.
+
+    python tests/golden/make_fixtures.py            # key files only (no reference needed)
+    python tests/golden/make_fixtures.py --golden   # + golden vectors from oracle/_ref
+
+Key files (tests/golden/keys/) use the reference's key-file format
+(etoheom-cpu/lib/param.cpp:102-332).  The ETO bath lines were fitted once with
+eto-heom_b200/etofit.py (a restatement of etom/ohmic_ETOM.py) and are frozen below,
+because curve_fit results move with the scipy version.
+
+Interpretation recorded here: "2 ETO modes per site" = one fitted oscillator = two
+BATH lines (+w, -w) per site, which reproduces the ADO counts 70 / 680 / 2925 / 210.
+The "perturbative amplitude 1e-4 in dipole units" is E0 = 0.5308 cm^-1, so that
+E0 * |mu| / hbar = 1e-4 fs^-1 for a unit dipole.
+
+Golden vectors (tests/golden/ref/*.npz) are the reference's own code -- its
+etoheom-cpu/lib sources compiled unmodified against the GSL-API shim
+(oracle/Makefile `ref` target) and driven by oracle/ref_driver.cpp -- printed at
+full precision.  Synthetic systems stand in for a public dataset (the reference
+has none); every random choice comes from a fixed numpy seed.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+KEYS = os.path.join(HERE, "keys")
+REF = os.path.join(HERE, "ref")
+ROOT = os.path.dirname(os.path.dirname(HERE))
+
+# Frozen ETO fits (etofit.ohmic / etofit.superohmic, one oscillator -> two lines).
+OHMIC_35_106_77K = ("0.006593820648078373", [
+    "0.00010950 -0.00005111 0.02549399 0.00000001",
+    "0.00010950 -0.00005111 0.02549399 -0.00000001"])
+SUPEROHMIC_50_150_300K = ("0.009419743782969104", [
+    "0.00019549 -0.00007598 0.04532376 0.08233007",
+    "0.00019549 -0.00007598 0.04532376 -0.08233007"])
+# The reference's own example bath (example/CPU_dimer_ohmic/key.key-tmpl:25-33).
+REF_EXAMPLE_BATH = ("0.008995192714312095", [
+    "0.00311213 -0.00252971 0.12340683 0.00000006",
+    "0.00311213 -0.00252971 0.12340683 -0.00000006",
+    "-0.00296194 0.00259667 0.12950563 0.02683512",
+    "-0.00296194 0.00259667 0.12950563 -0.02683512",
+    "0.00001177 -0.00003282 0.00754453 0.00000000",
+    "0.00001177 -0.00003282 0.00754453 -0.00000000"])
+
+E0 = "0.5308"
+
+
+def key_text(size, K, L, H, bath, dipoles, pulses, time, n_sample=1, seed=7, sigma=None,
+             single_manifold=False, extra=""):
+    """Render a key file.  H is the single_size x single_size block in cm^-1."""
+    sys_size = size if single_manifold else size + (size - 1) * (size - 2) // 2
+    out = ["# synthetic fixture (tests/golden/make_fixtures.py)", "SIZE", str(size), ""]
+    if single_manifold:
+        out += ["MANIFOLD", "single", ""]
+    out += ["HEOM", f"{K} {L}", "", "HAMILTONIAN"]
+    out += [" ".join(f"{v:.10g}" for v in row) for row in H]
+    out += ["", "DISORDER", f"{n_sample} {seed}"]
+    sig = np.zeros((size, size)) if sigma is None else np.asarray(sigma)
+    out += [" ".join(f"{v:.10g}" for v in row) for row in sig]
+    out += [""] * (sys_size - size)  # the CPU parser reads sys_size rows (param.cpp:145)
+    out += ["", "TEMPERATURE", "77", "", "BATH", bath[0], str(len(bath[1]))] + list(bath[1])
+    out += ["", "DIPOLE", str(len(dipoles))]
+    out += [f"{i} {j} {x:.10g} {y:.10g} {z:.10g}" for i, j, x, y, z in dipoles]
+    out += ["", "POLARIZATION", "0 0 0 0", "", "PULSE", "3"]
+    out += [f"{E0} {tau:g} {taup:g} {w:g}" for tau, taup, w in pulses]
+    out += ["", "TIME", " ".join(f"{v:g}" for v in time)]
+    if extra:
+        out += ["", extra]
+    return "\n".join(out) + "\n"
+
+
+def dimer_H():
+    return [[0, 0, 0], [0, 12400, 100], [0, 100, 12600]]
+
+
+def dimer_key(tau=(50, 150, 250), t_end=1000, dt=0.5, pstep=0.5, **kw):
+    return key_text(3, 2, 4, dimer_H(), OHMIC_35_106_77K,
+                    [(0, 1, 0.0, 0.0, 1.0), (0, 2, 0.0, 0.0, 1.0)],
+                    [(t, 20, 12500) for t in tau], (0, t_end, dt, pstep), **kw)
+
+
+def aggregate(n_sites, seed, e_mean, e_sd, j_max, e_fixed=None):
+    rng = np.random.default_rng(seed)
+    e = np.array(e_fixed, float) if e_fixed is not None else rng.normal(e_mean, e_sd, n_sites)
+    H = np.zeros((n_sites + 1, n_sites + 1))
+    for a in range(n_sites):
+        H[a + 1, a + 1] = round(float(e[a]), 4)
+    for a in range(n_sites):
+        for b in range(a + 1, n_sites):
+            j = round(float(rng.uniform(-j_max, j_max)), 4)
+            H[a + 1, b + 1] = H[b + 1, a + 1] = j
+    mu = rng.normal(0, 1, (n_sites, 3))
+    mu /= np.linalg.norm(mu, axis=1, keepdims=True)
+    dip = [(0, a + 1, *map(float, np.round(mu[a], 6))) for a in range(n_sites)]
+    return H.tolist(), dip
+
+
+def chain(n_sites, seed, e_sd, j_nn):
+    rng = np.random.default_rng(seed)
+    e = rng.normal(12400, e_sd, n_sites)
+    H = np.zeros((n_sites + 1, n_sites + 1))
+    for a in range(n_sites):
+        H[a + 1, a + 1] = round(float(e[a]), 4)
+        if a + 1 < n_sites:
+            H[a + 1, a + 2] = H[a + 2, a + 1] = j_nn
+    mu = rng.normal(0, 1, (n_sites, 3))
+    mu /= np.linalg.norm(mu, axis=1, keepdims=True)
+    return H.tolist(), [(0, a + 1, *map(float, np.round(mu[a], 6))) for a in range(n_sites)]
+
+
+def scan_points(t0=50.0, t1_step=5.0, n_t1=64, t2_step=100.0, n_t2=8, t3=400.0):
+    """The 2DES delay scan: (tau1, tau2, tau3, t_end, kind) for every point.
+    Rephasing: pulse 1 first; non-rephasing: pulse 2 first (gen_2d_data.sh:37-61)."""
+    pts = []
+    for kind in ("R", "NR"):
+        for i2 in range(n_t2):
+            for i1 in range(n_t1):
+                t1, t2 = i1 * t1_step, i2 * t2_step
+                if kind == "R":
+                    tau = (t0, t0 + t1, t0 + t1 + t2)
+                else:
+                    tau = (t0 + t1, t0, t0 + t1 + t2)
+                pts.append((tau[0], tau[1], tau[2], tau[2] + t3, kind))
+    return pts
+
+
+def write_keys():
+    os.makedirs(KEYS, exist_ok=True)
+    files = {}
+    # c0: dimer, L=4, 2001 steps.
+    files["c0_dimer.key"] = dimer_key()
+    files["c0_dimer_short.key"] = dimer_key(t_end=300)
+    # c2 scan template (TAU1..3 / T_END substituted per point, as the reference's
+    # script/IO-scripts/key.key-tmpl).
+    files["c2_dimer_scan.key-tmpl"] = (dimer_key().replace("50 20 12500", "TAU1 20 12500", 1)
+                                       .replace("150 20 12500", "TAU2 20 12500", 1)
+                                       .replace("250 20 12500", "TAU3 20 12500", 1)
+                                       .replace("0 1000 0.5 0.5", "0 T_END 0.5 0.5"))
+    # c1: 7-site FMO-like aggregate with the two-exciton manifold, N=29, L=3.
+    H, dip = aggregate(7, 2024, 12400, 200, 100)
+    files["c1_fmo.key"] = key_text(8, 7, 3, H, OHMIC_35_106_77K, dip,
+                                   [(50, 20, 12500), (150, 20, 12500), (250, 20, 12500)], (0, 2000, 0.5, 0.5))
+    files["c1_fmo_short.key"] = key_text(8, 7, 3, H, OHMIC_35_106_77K, dip,
+                                         [(0, 20, 12500), (1, 20, 12500), (0, 20, 12500)], (0, 3, 0.5, 0.5))
+    # c3: 12-site chain, single-excitation manifold (extension keyword), L=3.
+    H, dip = chain(12, 77, 150, 80)
+    files["c3_chain.key"] = key_text(13, 12, 3, H, SUPEROHMIC_50_150_300K, dip,
+                                     [(50, 20, 12500)] * 3, (0, 3000, 0.5, 0.5), single_manifold=True)
+    files["c3_chain_short.key"] = key_text(13, 12, 3, H, SUPEROHMIC_50_150_300K, dip,
+                                           [(0, 20, 12500)] * 3, (0, 10, 0.5, 0.5), single_manifold=True)
+    # c4: trimer with two-exciton manifold (N=7), L=4.
+    H, dip = aggregate(3, 4, 0, 0, 120, e_fixed=[12300, 12450, 12600])
+    files["c4_trimer.key"] = key_text(4, 3, 4, H, OHMIC_35_106_77K, dip,
+                                      [(50, 20, 12500), (150, 20, 12500), (350, 20, 12500)], (0, 1000, 0.5, 0.5))
+    files["c4_trimer_short.key"] = key_text(4, 3, 4, H, OHMIC_35_106_77K, dip,
+                                            [(20, 20, 12500), (50, 20, 12500), (80, 20, 12500)], (0, 160, 0.5, 0.5))
+    # Disorder + several samples: exercises the RNG stream, the diagonal sort and averaging.
+    files["t_disorder.key"] = dimer_key(tau=(30, 60, 90), t_end=140, n_sample=3, seed=114,
+                                        sigma=[[0, 0, 0], [0, 42.4, 0], [0, 0, 42.4]])
+    # The reference's own example system (example/CPU_dimer_ohmic/key.key-tmpl), K=2, L=2,
+    # 6 bath lines (91 ADOs), dt = 2 fs, print every 10 fs, two samples.
+    files["t_ref_example.key"] = key_text(3, 2, 2, [[0, 0, 0], [0, 400, 100], [0, 100, 500]], REF_EXAMPLE_BATH,
+                                          [(0, 1, 1.0, 0.0, 0.0), (0, 2, 0.0, 1.0, 0.0)],
+                                          [(210, 20, 500), (260, 20, 500), (260, 20, 500)], (0, 900, 2, 10),
+                                          n_sample=2, seed=114,
+                                          sigma=[[0, 0, 0], [0, 42.4, 0], [0, 0, 42.4]])
+    # Large first-order field (no perturbative smallness) and a negative site energy,
+    # which the reference's diagonal sort treats specially (dynamics.cpp:24-27).
+    files["t_strong.key"] = key_text(3, 2, 3, [[0, 0, 0], [0, -50, 300], [0, 300, 400]], OHMIC_35_106_77K,
+                                     [(0, 1, 0.3, -0.2, 0.9), (0, 2, 0.5, 0.1, -0.8)],
+                                     [(10, 8, 200), (30, 8, 200), (45, 8, 200)], (0, 80, 0.25, 0.5))
+    for name, text in files.items():
+        with open(os.path.join(KEYS, name), "w") as f:
+            f.write(text)
+    return sorted(files)
+
+
+def parse_driver_output(text):
+    """Parse ref_driver / heom_oracle output into (traj[n_sample, 3, n], combined[n])."""
+    trajs, comb, cur, mode = [], [], None, None
+    for line in text.splitlines():
+        if line.startswith("#traj"):
+            cur = []
+            trajs.append(cur)
+            mode = "t"
+        elif line.startswith("#combined"):
+            mode = "c"
+        elif line.startswith("#"):
+            mode = None
+        elif mode == "t":
+            v = [float(x) for x in line.split()]
+            cur.append([complex(v[0], v[1]), complex(v[2], v[3]), complex(v[4], v[5])])
+        elif mode == "c":
+            v = [float(x) for x in line.split()]
+            comb.append(complex(v[0], v[1]))
+    traj = np.array([np.array(t).T for t in trajs], dtype=np.complex128) if trajs else np.zeros((0, 3, 0))
+    return traj, np.array(comb, dtype=np.complex128)
+
+
+GOLDEN = ["c0_dimer_short.key", "c0_dimer.key", "c4_trimer_short.key", "t_disorder.key",
+          "t_ref_example.key", "t_strong.key", "c1_fmo_short.key"]
+
+
+def write_golden():
+    drv = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    if not os.path.exists(drv):
+        subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "ref"])
+    os.makedirs(REF, exist_ok=True)
+    for name in GOLDEN:
+        out = subprocess.run([drv, os.path.join(KEYS, name)], check=True, capture_output=True, text=True).stdout
+        traj, comb = parse_driver_output(out)
+        np.savez_compressed(os.path.join(REF, name.replace(".key", ".npz")), traj=traj, combined=comb)
+        print(f"{name}: traj {traj.shape} combined {comb.shape}")
+    # The unmodified CPU_2DES executable's stdout, for byte-compatibility of the CLI.
+    exe = os.path.join(ROOT, "oracle", "_ref", "CPU_2DES")
+    for name in ["c0_dimer_short.key", "t_disorder.key"]:
+        out = subprocess.run([exe, os.path.join(KEYS, name)], check=True, capture_output=True, text=True).stdout
+        with open(os.path.join(REF, name.replace(".key", ".out")), "w") as f:
+            f.write(out)
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--golden", action="store_true")
+    a = ap.parse_args()
+    print("\n".join(write_keys()))
+    if a.golden:
+        write_golden()
