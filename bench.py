@@ -349,14 +349,35 @@ def run_ours(a):
     return out
 
 
+def profile_run(precision: str):
+    """A small case of the same kernel for profiler captures: the first 148 points of
+    the scan (one per SM) with t3 shortened to 50 fs, default launch shape, one run."""
+    import torch
+
+    from heomtest import load_pkg
+
+    heom = load_pkg()
+    prob = heom.Problem.from_key(KEY)
+    prob.prepare_sample()
+    rows = [(a, b, c, c + 50.0) for a, b, c, _ in scan_rows()[:148]]
+    plan = heom.Plan(prob, precision, max_points=len(rows))
+    r = plan.run_scan(heom.make_points(rows))
+    torch.cuda.synchronize()
+    print(f"profile run: {len(rows)} points, {len(r.P)} P values, {plan.describe()}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--profile-run", default=None, choices=["fp32-bulk", "fp64"],
+                    help="run only a small scan of that precision (for profiler captures)")
     a = ap.parse_args()
-    if a.impl == "reference":
+    if a.profile_run:
+        profile_run(a.profile_run)
+    elif a.impl == "reference":
         run_reference_arm(a)
     else:
         run_ours(a)

@@ -213,7 +213,6 @@ __global__ void __launch_bounds__(MAXT, 1) scan_kernel(ScanArgs a) {
     const int pi = a.use_order ? a.order[idx] : idx;
     const heom_scan_point pt = a.pts[pi];
     const long long off = a.offsets[pi];
-    const double tau[3] = {pt.tau1, pt.tau2, pt.tau3};
     // float nstep and the i <= nstep loop bound of dynamics.cpp:344-347
     const float nstep = (pt.t_end - a.t_start) / a.dt;
     const int nsteps = nstep >= 0.0f ? (int)nstep + 1 : 0;
@@ -232,7 +231,7 @@ __global__ void __launch_bounds__(MAXT, 1) scan_kernel(ScanArgs a) {
     for (int i = 0; i < nsteps; i++) {
       if (tid < 3) {
         const int q = tid;
-        const double d = (double)t - tau[q];
+        const double d = (double)t - (q == 0 ? pt.tau1 : q == 1 ? pt.tau2 : pt.tau3);
         const int on = fabs(d) <= a.taup[q] * 2;
         double2 ef = make_double2(0.0, 0.0);
         if (on) {
@@ -266,7 +265,7 @@ __global__ void __launch_bounds__(MAXT, 1) scan_kernel(ScanArgs a) {
         A[5 * NN + q] = mk2<T>(r3, i3);
       }
       // record P = Tr(X3 (Q - R)) on ADO 0 before the step (dynamics.cpp:367-381)
-      if (t >= tau[2] && i % a.stride == 0) {
+      if (t >= pt.tau3 && i % a.stride == 0) {
         if (tid < 32) {
           double sr = 0.0, si = 0.0;
           const int qbase = 3 * nado * NN;
@@ -380,6 +379,337 @@ __global__ void __launch_bounds__(MAXT, 1) scan_kernel(ScanArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Row-block form for a compile-time system size NT.  Each thread owns RPT rows of one
+// (component, ADO) block.  Per stage it loads that block's FP32 copy once (vector
+// loads), keeps its component's operator A in registers (reloaded once per step), and
+// keeps its FP64 Horner accumulator w in registers: only the FP32 copy of w is shared,
+// double-buffered so one barrier per stage suffices.
+template <int NT> __host__ __device__ inline size_t rows_smem_bytes(size_t tsz, int n_ado, int M, int K_m, int E) {
+  constexpr int NN = NT * NT;
+  const size_t nM = (size_t)n_ado * M;
+  size_t b = 0;
+  b += 16 * (size_t)E;               // rho (FP64)
+  b += 2 * 2 * tsz * (size_t)E;      // w copies in contraction precision, double-buffered
+  b += al16(2 * tsz * 6 * NN);       // A[4], S2, S3
+  b += al16(16 * (size_t)NN);        // X3
+  b += al16(8 * (size_t)NN);         // Hd[r] - Hd[c]
+  b += al16(16 * (size_t)n_ado);     // damp
+  b += al16(2 * tsz * K_m);          // alpha
+  b += al16(tsz * nM) * 2;           // x, y
+  b += al16(2 * nM) * 2;             // up, dn
+  return b;
+}
+
+template <class T2, int NT> __device__ __forceinline__ void load_row(T2 (&dst)[NT], const T2 *src) {
+#pragma unroll
+  for (int c = 0; c < NT; c++) dst[c] = src[c];
+}
+
+template <typename T, int NT, int RPT, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) scan_rows(ScanArgs a) {
+  using T2 = typename V2<T>::t;
+  constexpr int NN = NT * NT, GPR = NT / RPT;
+  static_assert(NT % RPT == 0, "rows per thread must divide N");
+  extern __shared__ __align__(16) unsigned char sm[];
+  __shared__ double2 s_field[3];
+  __shared__ int s_on[3], s_point;
+  const int E = a.E, M = a.M, nado = a.n_ado, K = a.K, Km = a.K_m;
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const size_t nM = (size_t)nado * M;
+  unsigned char *p = sm;
+  double2 *rho = (double2 *)p;
+  p += 16 * (size_t)E;
+  T2 *w32 = (T2 *)p;                   // [2][E]
+  p += 2 * sizeof(T2) * (size_t)E;
+  T2 *Aall = (T2 *)p;
+  p += al16(sizeof(T2) * 6 * NN);
+  double2 *X3 = (double2 *)p;
+  p += al16(16 * (size_t)NN);
+  double *Hdd = (double *)p;
+  p += al16(8 * (size_t)NN);
+  double2 *damp = (double2 *)p;
+  p += al16(16 * (size_t)nado);
+  T2 *alpha = (T2 *)p;
+  p += al16(sizeof(T2) * Km);
+  T *xc = (T *)p;
+  p += al16(sizeof(T) * nM);
+  T *yc = (T *)p;
+  p += al16(sizeof(T) * nM);
+  short *up = (short *)p;
+  p += al16(2 * nM);
+  short *dn = (short *)p;
+  TableLayout tl(nado, M, Km);
+  const short *g_up = (const short *)(a.tables + tl.up), *g_dn = (const short *)(a.tables + tl.dn);
+  const double *g_x = (const double *)(a.tables + tl.x), *g_y = (const double *)(a.tables + tl.y);
+  const double2 *g_damp = (const double2 *)(a.tables + tl.damp), *g_alpha = (const double2 *)(a.tables + tl.alpha);
+  for (size_t q = tid; q < nM; q += bs) {
+    up[q] = g_up[q];
+    dn[q] = g_dn[q];
+    xc[q] = (T)g_x[q];
+    yc[q] = (T)g_y[q];
+  }
+  for (int q = tid; q < nado; q += bs) damp[q] = g_damp[q];
+  for (int q = tid; q < Km; q += bs) alpha[q] = mk2<T>(g_alpha[q].x, g_alpha[q].y);
+  const double *g_Hd = a.sys, *g_Hoff = a.sys + NT, *g_Xs = g_Hoff + 2 * NN, *g_X3 = g_Xs + 6 * NN;
+  for (int q = tid; q < NN; q += bs) {
+    X3[q] = make_double2(g_X3[2 * q], g_X3[2 * q + 1]);
+    Hdd[q] = g_Hd[q / NT] - g_Hd[q % NT];
+  }
+  const int ntask = 4 * nado * GPR;
+  const bool active = tid < ntask;
+  int cc = 0, n = 0, r0 = 0;
+  if (active) {
+    cc = tid / (nado * GPR);
+    const int rem = tid - cc * nado * GPR;
+    n = rem / GPR;
+    r0 = (rem - n * GPR) * RPT;
+  }
+  const int base = (cc * nado + n) * NN;
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_point = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int idx = s_point;
+    if (idx >= a.n_points) break;
+    const int pi = a.use_order ? a.order[idx] : idx;
+    const heom_scan_point pt = a.pts[pi];
+    const long long off = a.offsets[pi];
+    const float nstep = (pt.t_end - a.t_start) / a.dt;
+    const int nsteps = nstep >= 0.0f ? (int)nstep + 1 : 0;
+    double2 w64[RPT][NT];
+    if (active) {
+#pragma unroll
+      for (int rr = 0; rr < RPT; rr++)
+#pragma unroll
+        for (int c = 0; c < NT; c++) {
+          const int e = base + (r0 + rr) * NT + c;
+          const double v = e == 0 ? 1.0 : 0.0;
+          w64[rr][c] = make_double2(v, 0.0);
+          rho[e] = w64[rr][c];
+          w32[e] = mk2<T>(v, 0.0);
+        }
+    }
+    int buf = 0;
+    float t = a.t_start;
+    int rec = 0;
+    for (int i = 0; i < nsteps; i++) {
+      if (tid < 3) {
+        const int q = tid;
+        const double d = (double)t - (q == 0 ? pt.tau1 : q == 1 ? pt.tau2 : pt.tau3);
+        const int on = fabs(d) <= a.taup[q] * 2;
+        double2 ef = make_double2(0.0, 0.0);
+        if (on) {
+          const double Eq = a.E0[q] * exp(-2.77 * d * d / a.taup[q] / a.taup[q]);
+          double sn, cs;
+          sincos(q == 0 ? a.w0[q] * d : -a.w0[q] * d, &sn, &cs);
+          ef = make_double2(Eq * cs, Eq * sn);
+        }
+        s_on[q] = on;
+        s_field[q] = ef;
+      }
+      __syncthreads();
+      const int on1 = s_on[0], on2 = s_on[1], on3 = s_on[2];
+      for (int q = tid; q < NN; q += bs) {
+        double vr[3], vi[3];
+        for (int s = 0; s < 3; s++) {
+          const double xr = g_Xs[2 * (s * NN + q)], xi = g_Xs[2 * (s * NN + q) + 1];
+          const double2 ef = s_field[s];
+          vr[s] = -(xr * ef.x - xi * ef.y);
+          vi[s] = -(xr * ef.y + xi * ef.x);
+        }
+        const double br = g_Hoff[2 * q] + (on1 ? vr[0] : 0.0), bi = g_Hoff[2 * q + 1] + (on1 ? vi[0] : 0.0);
+        const double r2 = on2 ? vr[1] : 0.0, i2 = on2 ? vi[1] : 0.0, r3 = on3 ? vr[2] : 0.0, i3 = on3 ? vi[2] : 0.0;
+        Aall[q] = mk2<T>(br, bi);
+        Aall[NN + q] = mk2<T>(br + r2, bi + i2);
+        Aall[2 * NN + q] = mk2<T>(br + r3, bi + i3);
+        Aall[3 * NN + q] = mk2<T>(br + r2 + r3, bi + i2 + i3);
+        Aall[4 * NN + q] = mk2<T>(r2, i2);
+        Aall[5 * NN + q] = mk2<T>(r3, i3);
+      }
+      if (t >= pt.tau3 && i % a.stride == 0) {
+        if (tid < 32) {
+          double sr = 0.0, si = 0.0;
+          const int qbase = 3 * nado * NN;
+          for (int q = tid; q < NN; q += 32) {
+            const int jr = q / NT, l = q - jr * NT;
+            const double2 qv = rho[qbase + q], rv = rho[q], x = X3[l * NT + jr];
+            const double dr = qv.x - rv.x, di = qv.y - rv.y;
+            sr += dr * x.x - di * x.y;
+            si += dr * x.y + di * x.x;
+          }
+          for (int o = 16; o > 0; o >>= 1) {
+            sr += __shfl_down_sync(0xffffffffu, sr, o);
+            si += __shfl_down_sync(0xffffffffu, si, o);
+          }
+          if (tid == 0) a.P[off + rec] = make_double2(sr, si);
+        }
+        rec++;
+      }
+      __syncthreads();
+      const T2 *Ac = Aall + cc * NN;
+      const bool src = (on2 || on3) && cc > 0;
+      for (int m = 4; m >= 1; m--) {
+        const double cm = a.h / m;
+        const T2 *W = w32 + (size_t)buf * E;
+        T2 *Wn = w32 + (size_t)(buf ^ 1) * E;
+        if (active) {
+          // X = A w - w A, streaming row l of w and of A from shared memory; the
+          // thread's own row entries A[r][l], w[r][l] are loaded per l so that every
+          // register array is indexed by compile-time constants only.
+          T xr[RPT][NT], xi[RPT][NT];
+#pragma unroll
+          for (int rr = 0; rr < RPT; rr++)
+#pragma unroll
+            for (int c = 0; c < NT; c++) { xr[rr][c] = 0; xi[rr][c] = 0; }
+#pragma unroll
+          for (int l = 0; l < NT; l++) {
+            T2 wl[NT], al[NT];
+            load_row<T2, NT>(wl, W + base + l * NT);
+            load_row<T2, NT>(al, Ac + l * NT);
+#pragma unroll
+            for (int rr = 0; rr < RPT; rr++) {
+              const T2 a1 = Ac[(r0 + rr) * NT + l], z2 = W[base + (r0 + rr) * NT + l];
+#pragma unroll
+              for (int c = 0; c < NT; c++) {
+                const T2 z1 = wl[c], a2 = al[c];
+                T sr = xr[rr][c], si = xi[rr][c];
+                sr = fma(a1.x, z1.x, sr);
+                sr = fma(-a1.y, z1.y, sr);
+                si = fma(a1.x, z1.y, si);
+                si = fma(a1.y, z1.x, si);
+                sr = fma(-z2.x, a2.x, sr);
+                sr = fma(z2.y, a2.y, sr);
+                si = fma(-z2.x, a2.y, si);
+                si = fma(-z2.y, a2.x, si);
+                xr[rr][c] = sr;
+                xi[rr][c] = si;
+              }
+            }
+          }
+          if (src) {
+            // sources: D2 <- P2 R, D3 <- P3 R, Q <- P2 D3 + P3 D2
+#pragma unroll 1
+            for (int s2 = 0; s2 < 2; s2++) {
+              int from = -1, op = 0;
+              if (cc == 1 && s2 == 0 && on2) { from = 0; op = 4; }
+              if (cc == 2 && s2 == 0 && on3) { from = 0; op = 5; }
+              if (cc == 3 && s2 == 0 && on2) { from = 2; op = 4; }
+              if (cc == 3 && s2 == 1 && on3) { from = 1; op = 5; }
+              if (from < 0) continue;
+              const T2 *S = Aall + op * NN;
+              const T2 *Wf = W + (from * nado + n) * NN;
+#pragma unroll
+              for (int rr = 0; rr < RPT; rr++)
+#pragma unroll
+                for (int c = 0; c < NT; c++) {
+                  const int r = r0 + rr;
+                  T sr = xr[rr][c], si = xi[rr][c];
+#pragma unroll
+                  for (int l = 0; l < NT; l++) {
+                    const T2 al = S[r * NT + l], wl = Wf[l * NT + c], wr = Wf[r * NT + l], ar = S[l * NT + c];
+                    sr = fma(al.x, wl.x, sr);
+                    sr = fma(-al.y, wl.y, sr);
+                    si = fma(al.x, wl.y, si);
+                    si = fma(al.y, wl.x, si);
+                    sr = fma(-wr.x, ar.x, sr);
+                    sr = fma(wr.y, ar.y, sr);
+                    si = fma(-wr.x, ar.y, si);
+                    si = fma(-wr.y, ar.x, si);
+                  }
+                  xr[rr][c] = sr;
+                  xi[rr][c] = si;
+                }
+            }
+          }
+          // k32 = -i X, then the one-hot bath couplings (dynamics.cpp:143-179)
+          T kr[RPT][NT], ki[RPT][NT];
+#pragma unroll
+          for (int rr = 0; rr < RPT; rr++)
+#pragma unroll
+            for (int c = 0; c < NT; c++) { kr[rr][c] = xi[rr][c]; ki[rr][c] = -xr[rr][c]; }
+#pragma unroll
+          for (int rr = 0; rr < RPT; rr++) {
+            const int r = r0 + rr;
+            if (r >= 1 && r <= K) { // row pass: s = r
+              const int j = r - 1;
+              for (int k = 0; k < Km; k++) {
+                const int o = n * M + j + k * K;
+                const int u = up[o], d = dn[o];
+                if (u >= 0) {
+                  const T x = xc[o];
+                  T2 z[NT];
+                  load_row<T2, NT>(z, W + (cc * nado + u) * NN + r * NT);
+#pragma unroll
+                  for (int c = 0; c < NT; c++)
+                    if (c != r) { kr[rr][c] = fma(-x, z[c].y, kr[rr][c]); ki[rr][c] = fma(x, z[c].x, ki[rr][c]); }
+                }
+                if (d >= 0) {
+                  const T y = yc[o];
+                  const T2 al = alpha[k];
+                  const T br = -al.y * y, ai = al.x * y;
+                  T2 z[NT];
+                  load_row<T2, NT>(z, W + (cc * nado + d) * NN + r * NT);
+#pragma unroll
+                  for (int c = 0; c < NT; c++) {
+                    const T cr = c == r ? 2 * br : br, ci = c == r ? (T)0 : ai;
+                    kr[rr][c] = fma(cr, z[c].x, fma(-ci, z[c].y, kr[rr][c]));
+                    ki[rr][c] = fma(cr, z[c].y, fma(ci, z[c].x, ki[rr][c]));
+                  }
+                }
+              }
+            }
+#pragma unroll
+            for (int c = 1; c < NT; c++) { // column pass: s = c != r
+              if (c > K || c == r) continue;
+              const int j = c - 1;
+              for (int k = 0; k < Km; k++) {
+                const int o = n * M + j + k * K;
+                const int u = up[o], d = dn[o];
+                if (u >= 0) {
+                  const T x = xc[o];
+                  const T2 z = W[(cc * nado + u) * NN + r * NT + c];
+                  kr[rr][c] = fma(x, z.y, kr[rr][c]);
+                  ki[rr][c] = fma(-x, z.x, ki[rr][c]);
+                }
+                if (d >= 0) {
+                  const T y = yc[o];
+                  const T2 al = alpha[k];
+                  const T cr = -al.y * y, ci = -al.x * y;
+                  const T2 z = W[(cc * nado + d) * NN + r * NT + c];
+                  kr[rr][c] = fma(cr, z.x, fma(-ci, z.y, kr[rr][c]));
+                  ki[rr][c] = fma(cr, z.y, fma(ci, z.x, ki[rr][c]));
+                }
+              }
+            }
+          }
+          // FP64: damping and site-energy diagonal, Horner update
+          const double2 dmp = damp[n];
+#pragma unroll
+          for (int rr = 0; rr < RPT; rr++)
+#pragma unroll
+            for (int c = 0; c < NT; c++) {
+              const int r = r0 + rr, e = base + r * NT + c;
+              const double gr = dmp.x, gi = dmp.y - Hdd[r * NT + c];
+              const double2 wv = w64[rr][c];
+              const double k_r = fma(gr, wv.x, fma(-gi, wv.y, (double)kr[rr][c]));
+              const double k_i = fma(gr, wv.y, fma(gi, wv.x, (double)ki[rr][c]));
+              const double2 r0v = rho[e];
+              const double2 wn = make_double2(fma(cm, k_r, r0v.x), fma(cm, k_i, r0v.y));
+              w64[rr][c] = wn;
+              Wn[e] = mk2<T>(wn.x, wn.y);
+              if (m == 1) rho[e] = wn;
+            }
+        }
+        buf ^= 1;
+        __syncthreads();
+      }
+      t += a.dt;
+    }
+  }
+}
+
 // Order points by descending step count (single CTA, bitonic sort in shared memory).
 __global__ void scan_order(const heom_scan_point *pts, int n, float t_start, float dt, int *order, int *counter) {
   extern __shared__ unsigned long long keys[];
@@ -418,32 +748,57 @@ namespace {
 
 using KernelFn = void (*)(ScanArgs);
 
+// Launch shapes the autotuner chooses from.  rows_nt > 0: row-block form for that
+// compile-time N with `per` rows per thread; rows_nt == 0: element form (any N) with
+// `per` elements per thread.
 struct Variant {
-  int ept, maxt;
+  int rows_nt, per, maxt;
   KernelFn f32, f64;
 };
 
 const Variant kVariants[] = {
-    {2, 1024, scan_kernel<float, 2, 1024>, scan_kernel<double, 2, 1024>},
-    {4, 1024, scan_kernel<float, 4, 1024>, scan_kernel<double, 4, 1024>},
-    {5, 1024, scan_kernel<float, 5, 1024>, scan_kernel<double, 5, 1024>},
-    {6, 768, scan_kernel<float, 6, 768>, scan_kernel<double, 6, 768>},
-    {8, 640, scan_kernel<float, 8, 640>, scan_kernel<double, 8, 640>},
-    {12, 512, scan_kernel<float, 12, 512>, scan_kernel<double, 12, 512>},
-    {16, 384, scan_kernel<float, 16, 384>, scan_kernel<double, 16, 384>},
+    {4, 1, 1024, scan_rows<float, 4, 1, 1024>, scan_rows<double, 4, 1, 1024>},
+    {4, 2, 640, scan_rows<float, 4, 2, 640>, scan_rows<double, 4, 2, 640>},
+    {4, 4, 320, scan_rows<float, 4, 4, 320>, scan_rows<double, 4, 4, 320>},
+    {0, 2, 1024, scan_kernel<float, 2, 1024>, scan_kernel<double, 2, 1024>},
+    {0, 4, 1024, scan_kernel<float, 4, 1024>, scan_kernel<double, 4, 1024>},
+    {0, 5, 1024, scan_kernel<float, 5, 1024>, scan_kernel<double, 5, 1024>},
+    {0, 6, 768, scan_kernel<float, 6, 768>, scan_kernel<double, 6, 768>},
+    {0, 8, 640, scan_kernel<float, 8, 640>, scan_kernel<double, 8, 640>},
+    {0, 12, 512, scan_kernel<float, 12, 512>, scan_kernel<double, 12, 512>},
+    {0, 16, 384, scan_kernel<float, 16, 384>, scan_kernel<double, 16, 384>},
 };
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
-const Variant *find_variant(int ept) {
-  for (const Variant &v : kVariants)
-    if (v.ept == ept) return &v;
-  return nullptr;
+int threads_for(const ScanState &s, const Variant &v) {
+  const int work = v.rows_nt ? 4 * s.n_ado * (s.N / v.per) : (s.E + v.per - 1) / v.per;
+  return (work + 31) / 32 * 32;
 }
 
-int threads_for(int E, int ept) { return ((E + ept - 1) / ept + 31) / 32 * 32; }
+size_t smem_for(const ScanState &s, const Variant &v) {
+  const bool d = s.precision == HEOM_FP64;
+  if (v.rows_nt == 4) return rows_smem_bytes<4>(d ? 8 : 4, s.n_ado, s.M, s.K_m, s.E);
+  return d ? scan_smem_bytes<double>(s.N, s.n_ado, s.M, s.K_m, s.E)
+           : scan_smem_bytes<float>(s.N, s.n_ado, s.M, s.K_m, s.E);
+}
 
-size_t smem_for(const ScanState &s) {
-  return s.precision == HEOM_FP64 ? scan_smem_bytes<double>(s.N, s.n_ado, s.M, s.K_m, s.E)
-                                  : scan_smem_bytes<float>(s.N, s.n_ado, s.M, s.K_m, s.E);
+bool feasible(const ScanState &s, const Variant &v, int max_smem) {
+  if (v.rows_nt && (v.rows_nt != s.N || s.N % v.per != 0)) return false;
+  const int th = threads_for(s, v);
+  return th >= 32 && th <= v.maxt && smem_for(s, v) + 1024 <= (size_t)max_smem;
+}
+
+// Shape, shared memory and a grid of every CTA that can be resident at once.
+void select_variant(ScanState &s, int vi) {
+  const Variant &v = kVariants[vi];
+  s.variant = vi;
+  s.ept = v.per;
+  s.threads = threads_for(s, v);
+  s.smem = smem_for(s, v);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s.precision == HEOM_FP64 ? v.f64 : v.f32, s.threads,
+                                                s.smem);
+  s.grid = s.sm_count * std::max(per_sm, 1);
 }
 
 ScanArgs make_args(const ScanState &s, const heom_scan_point *pts, int n, double *P, const long long *offsets,
@@ -482,7 +837,7 @@ cudaError_t enqueue(const ScanState &s, const heom_scan_point *d_pts, int n, dou
   } else {
     scan_reset<<<1, 1, 0, st>>>(s.d_counter);
   }
-  const Variant *v = find_variant(s.ept);
+  const Variant *v = &kVariants[s.variant];
   KernelFn f = s.precision == HEOM_FP64 ? v->f64 : v->f32;
   ScanArgs a = make_args(s, d_pts, n, d_P, d_off, sortable ? 1 : 0);
   const int grid = std::max(1, std::min(n, s.grid));
@@ -497,9 +852,11 @@ long long scan_launches_per_run(const ScanState &) { return 2; }
 std::string scan_describe(const ScanState &s) {
   if (!s.supported) return "unsupported (" + s.why + ")";
   char b[256];
-  std::snprintf(b, sizeof b, "%s, one CTA per point, %d threads x %d elements, %zu B smem, grid %d",
-                s.precision == HEOM_FP64 ? "fp64" : (s.precision == HEOM_FP32_BULK ? "fp32-bulk" : "fp64(scan)"),
-                s.threads, s.ept, s.smem, s.grid);
+  const Variant &v = kVariants[s.variant];
+  std::snprintf(b, sizeof b, "%s, one CTA per point, %d threads x %d %s, %zu B smem, grid %d%s",
+                s.precision == HEOM_FP64 ? "fp64" : "fp32-bulk", s.threads, v.per,
+                v.rows_nt ? "rows of one ADO block (N=4 form)" : "elements (generic form)", s.smem, s.grid,
+                s.tune_ms > 0 ? " (autotuned)" : "");
   return b;
 }
 
@@ -561,12 +918,14 @@ static int autotune(ScanState &s, const heom::Problem &p, cudaStream_t st) {
   cudaEventCreate(&e1);
   int best = -1;
   float best_ms = 1e30f;
-  for (const Variant &v : kVariants) {
-    const int th = threads_for(s.E, v.ept);
-    if (th > v.maxt || th < 32) continue;
+  int max_smem = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  for (int vi = 0; vi < kNumVariants; vi++) {
+    const Variant &v = kVariants[vi];
+    if (!feasible(s, v, max_smem)) continue;
     ScanState t = s;
-    t.ept = v.ept;
-    t.threads = th;
+    select_variant(t, vi);
     float ms_sum = 0;
     bool ok = true;
     for (int rep = 0; rep < 3 && ok; rep++) {
@@ -578,7 +937,7 @@ static int autotune(ScanState &s, const heom::Problem &p, cudaStream_t st) {
       cudaEventElapsedTime(&ms, e0, e1);
       if (rep > 0) ms_sum += ms;
     }
-    if (ok && ms_sum < best_ms) { best_ms = ms_sum; best = v.ept; }
+    if (ok && ms_sum < best_ms) { best_ms = ms_sum; best = vi; }
     cudaGetLastError();
   }
   cudaEventDestroy(e0);
@@ -587,8 +946,7 @@ static int autotune(ScanState &s, const heom::Problem &p, cudaStream_t st) {
   cudaFree(d_off);
   cudaFree(d_P);
   if (best < 0) { s_err = "autotune: no launch shape ran"; return HEOM_ERR_CUDA; }
-  s.ept = best;
-  s.threads = threads_for(s.E, best);
+  select_variant(s, best);
   s.tune_ms = best_ms / 2;
   return 0;
 }
@@ -613,27 +971,25 @@ int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_point
   cudaDeviceGetAttribute(&s.sm_count, cudaDevAttrMultiProcessorCount, dev);
   int max_smem = 0;
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  s.smem = smem_for(s);
-  if (s.N > 15 || s.n_ado >= 32768 || (long long)s.n_ado >= (1 << 20)) {
-    s.why = "scan kernel supports N <= 15";
+  if (s.N > 15 || s.n_ado >= 32768) {
+    s.why = "scan kernel supports N <= 15 and fewer than 32768 ADOs";
     return 0;
   }
-  if (s.smem + 64 > (size_t)max_smem) {
-    s.why = "state does not fit in shared memory (" + std::to_string(s.smem) + " B)";
+  // default shape: the first feasible variant (row-block forms come first)
+  s.variant = -1;
+  for (int vi = 0; vi < kNumVariants && s.variant < 0; vi++)
+    if (feasible(s, kVariants[vi], max_smem)) s.variant = vi;
+  if (s.variant < 0) {
+    s.why = "state does not fit in one CTA's shared memory (" +
+            std::to_string(smem_for(s, kVariants[kNumVariants - 1])) + " B)";
     return 0;
   }
-  // pick a feasible default shape: fewest elements per thread that fits
-  s.ept = -1;
-  for (const Variant &v : kVariants) {
-    const int th = threads_for(s.E, v.ept);
-    if (th <= v.maxt) { s.ept = v.ept; s.threads = th; break; }
-  }
-  if (s.ept < 0) { s.why = "too many elements per point for one CTA"; return 0; }
-  for (const Variant &v : kVariants) {
-    cudaFuncSetAttribute(v.f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-    cudaFuncSetAttribute(v.f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-  }
-  s.grid = s.sm_count; // one resident CTA per SM (shared memory bound)
+  for (const Variant &v : kVariants)
+    if (feasible(s, v, max_smem)) {
+      cudaFuncSetAttribute(v.f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_for(s, v));
+      cudaFuncSetAttribute(v.f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_for(s, v));
+    }
+  select_variant(s, s.variant);
   // tables
   TableLayout tl(p.n_ado, p.M, p.K_m);
   std::vector<unsigned char> tb(tl.total, 0);
@@ -680,7 +1036,7 @@ int scan_run_device(ScanState &s, const heom_scan_point *d_pts, int n, double *d
                     cudaStream_t st) {
   if (!s.supported) { s_err = "scan path unavailable for this problem: " + s.why; return HEOM_ERR_UNSUPPORTED; }
   if (n == 0) return 0;
-  const void *key[4] = {d_pts, d_P, d_offsets, (const void *)(size_t)s.ept};
+  const void *key[4] = {d_pts, d_P, d_offsets, (const void *)(size_t)(s.variant + 1)};
   if (!s.gexec || s.g_n != n || std::memcmp(key, s.g_key, sizeof key) != 0) {
     if (s.gexec) { cudaGraphExecDestroy(s.gexec); s.gexec = nullptr; }
     cudaGraph_t g;

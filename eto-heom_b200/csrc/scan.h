@@ -16,7 +16,7 @@ struct ScanState {
   bool supported = false;
   std::string why;
   // launch shape (autotuned)
-  int ept = 8, threads = 0, grid = 0, sm_count = 0;
+  int variant = 0, ept = 8, threads = 0, grid = 0, sm_count = 0;
   size_t smem = 0;
   float tune_ms = 0;
   // problem constants
