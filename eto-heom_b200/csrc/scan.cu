@@ -38,6 +38,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -710,6 +711,8 @@ __global__ void __launch_bounds__(MAXT, 1) scan_rows(ScanArgs a) {
   }
 }
 
+#include "scan_pm.cuh"
+
 // Order points by descending step count (single CTA, bitonic sort in shared memory).
 __global__ void scan_order(const heom_scan_point *pts, int n, float t_start, float dt, int *order, int *counter) {
   extern __shared__ unsigned long long keys[];
@@ -748,42 +751,52 @@ namespace {
 
 using KernelFn = void (*)(ScanArgs);
 
-// Launch shapes the autotuner chooses from.  rows_nt > 0: row-block form for that
-// compile-time N with `per` rows per thread; rows_nt == 0: element form (any N) with
-// `per` elements per thread.
+// Launch shapes the autotuner chooses from:
+//   kAdo  -- whole-ADO form, position-major shared layout (compile-time N = nt);
+//   kRows -- row-block form (compile-time N = nt, `per` rows per thread);
+//   kElem -- element form for any N (`per` elements per thread).
+enum Form { kAdo = 0, kRows = 1, kElem = 2 };
 struct Variant {
-  int rows_nt, per, maxt;
+  int form, nt, per, maxt;
   KernelFn f32, f64;
 };
 
 const Variant kVariants[] = {
-    {4, 1, 1024, scan_rows<float, 4, 1, 1024>, scan_rows<double, 4, 1, 1024>},
-    {4, 2, 640, scan_rows<float, 4, 2, 640>, scan_rows<double, 4, 2, 640>},
-    {4, 4, 320, scan_rows<float, 4, 4, 320>, scan_rows<double, 4, 4, 320>},
-    {0, 2, 1024, scan_kernel<float, 2, 1024>, scan_kernel<double, 2, 1024>},
-    {0, 4, 1024, scan_kernel<float, 4, 1024>, scan_kernel<double, 4, 1024>},
-    {0, 5, 1024, scan_kernel<float, 5, 1024>, scan_kernel<double, 5, 1024>},
-    {0, 6, 768, scan_kernel<float, 6, 768>, scan_kernel<double, 6, 768>},
-    {0, 8, 640, scan_kernel<float, 8, 640>, scan_kernel<double, 8, 640>},
-    {0, 12, 512, scan_kernel<float, 12, 512>, scan_kernel<double, 12, 512>},
-    {0, 16, 384, scan_kernel<float, 16, 384>, scan_kernel<double, 16, 384>},
+    {kAdo, 4, 4, 320, scan_pm<float, 4, 4, 320>, scan_pm<double, 4, 4, 320>},
+    {kAdo, 4, 2, 576, scan_pm<float, 4, 2, 576>, scan_pm<double, 4, 2, 576>},
+    {kAdo, 4, 2, 768, scan_pm<float, 4, 2, 768>, scan_pm<double, 4, 2, 768>},
+    {kAdo, 4, 1, 1024, scan_pm<float, 4, 1, 1024>, scan_pm<double, 4, 1, 1024>},
+    {kRows, 4, 1, 1024, scan_rows<float, 4, 1, 1024>, scan_rows<double, 4, 1, 1024>},
+    {kRows, 4, 2, 640, scan_rows<float, 4, 2, 640>, scan_rows<double, 4, 2, 640>},
+    {kRows, 4, 4, 320, scan_rows<float, 4, 4, 320>, scan_rows<double, 4, 4, 320>},
+    {kElem, 0, 2, 1024, scan_kernel<float, 2, 1024>, scan_kernel<double, 2, 1024>},
+    {kElem, 0, 4, 1024, scan_kernel<float, 4, 1024>, scan_kernel<double, 4, 1024>},
+    {kElem, 0, 5, 1024, scan_kernel<float, 5, 1024>, scan_kernel<double, 5, 1024>},
+    {kElem, 0, 6, 768, scan_kernel<float, 6, 768>, scan_kernel<double, 6, 768>},
+    {kElem, 0, 8, 640, scan_kernel<float, 8, 640>, scan_kernel<double, 8, 640>},
+    {kElem, 0, 12, 512, scan_kernel<float, 12, 512>, scan_kernel<double, 12, 512>},
+    {kElem, 0, 16, 384, scan_kernel<float, 16, 384>, scan_kernel<double, 16, 384>},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 int threads_for(const ScanState &s, const Variant &v) {
-  const int work = v.rows_nt ? 4 * s.n_ado * (s.N / v.per) : (s.E + v.per - 1) / v.per;
+  int work = 0;
+  if (v.form == kAdo || v.form == kRows) work = 4 * s.n_ado * (s.N / v.per);
+  else work = (s.E + v.per - 1) / v.per;
   return (work + 31) / 32 * 32;
 }
 
 size_t smem_for(const ScanState &s, const Variant &v) {
-  const bool d = s.precision == HEOM_FP64;
-  if (v.rows_nt == 4) return rows_smem_bytes<4>(d ? 8 : 4, s.n_ado, s.M, s.K_m, s.E);
-  return d ? scan_smem_bytes<double>(s.N, s.n_ado, s.M, s.K_m, s.E)
-           : scan_smem_bytes<float>(s.N, s.n_ado, s.M, s.K_m, s.E);
+  const size_t tsz = s.precision == HEOM_FP64 ? 8 : 4;
+  if (v.form == kAdo && v.nt == 4) return pm_smem_bytes<4>(tsz, s.n_ado, s.M, s.K_m, s.E);
+  if (v.form == kRows && v.nt == 4) return rows_smem_bytes<4>(tsz, s.n_ado, s.M, s.K_m, s.E);
+  return tsz == 8 ? scan_smem_bytes<double>(s.N, s.n_ado, s.M, s.K_m, s.E)
+                  : scan_smem_bytes<float>(s.N, s.n_ado, s.M, s.K_m, s.E);
 }
 
 bool feasible(const ScanState &s, const Variant &v, int max_smem) {
-  if (v.rows_nt && (v.rows_nt != s.N || s.N % v.per != 0)) return false;
+  if (v.form != kElem && v.nt != s.N) return false;
+  if (v.form != kElem && s.N % v.per != 0) return false;
   const int th = threads_for(s, v);
   return th >= 32 && th <= v.maxt && smem_for(s, v) + 1024 <= (size_t)max_smem;
 }
@@ -855,7 +868,10 @@ std::string scan_describe(const ScanState &s) {
   const Variant &v = kVariants[s.variant];
   std::snprintf(b, sizeof b, "%s, one CTA per point, %d threads x %d %s, %zu B smem, grid %d%s",
                 s.precision == HEOM_FP64 ? "fp64" : "fp32-bulk", s.threads, v.per,
-                v.rows_nt ? "rows of one ADO block (N=4 form)" : "elements (generic form)", s.smem, s.grid,
+                v.form == kAdo    ? "rows of one ADO block (N=4 form, position-major layout)"
+                : v.form == kRows ? "rows of one ADO block (N=4 form)"
+                                  : "elements (generic form)",
+                s.smem, s.grid,
                 s.tune_ms > 0 ? " (autotuned)" : "");
   return b;
 }
@@ -1024,6 +1040,14 @@ int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_point
   s.supported = true;
   int rc = scan_upload_system(s, p, st);
   if (rc) return rc;
+  // HEOM_SCAN_VARIANT=<index into the variant table> pins the launch shape (profiling).
+  if (const char *ev = std::getenv("HEOM_SCAN_VARIANT")) {
+    const int vi = std::atoi(ev);
+    if (vi >= 0 && vi < kNumVariants && feasible(s, kVariants[vi], max_smem)) {
+      select_variant(s, vi);
+      return 0;
+    }
+  }
   if (tune) {
     // tuning runs with the current (possibly zero) H and X; it only measures time
     rc = autotune(s, p, st);
