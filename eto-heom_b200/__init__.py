@@ -99,6 +99,7 @@ def lib() -> ctypes.CDLL:
         "heom_plan_launch_count": (ctypes.c_longlong, [P]),
         "heom_plan_destroy": (None, [P]),
         "heom_measure_fma_peak": (I, [I, I, D]),
+        "heom_run_scan_noalloc": (I, [P, I, P, I, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

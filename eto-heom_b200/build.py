@@ -32,6 +32,7 @@ UNITS = [
     ("exact.cu", ["--fmad=false"]),
     ("scan.cu", ["-Xptxas", "-warn-spills"]),
     ("peak.cu", []),
+    ("noalloc.cu", []),
 ]
 HEADERS = ["heom_host.h", "kernels.h", "exact.cuh", "scan.h"]
 

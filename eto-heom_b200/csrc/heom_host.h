@@ -92,4 +92,12 @@ Schedule make_schedule(const Problem &p, const double tau[3], float t_end, const
 int count_records(const Problem &p, double tau3, float t_end);
 int steps_for(const Problem &p, float t_end);
 
+// Sets the thread-local message returned by heom_last_error(); returns code.
+int set_error(int code, const std::string &msg);
+
 } // namespace heom
+
+// The opaque handle of the C ABI.
+struct heom_problem {
+  heom::Problem p;
+};

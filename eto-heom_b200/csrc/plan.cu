@@ -18,16 +18,17 @@
 #include "kernels.h"
 #include "scan.h"
 
-struct heom_problem {
-  heom::Problem p;
-};
-
 namespace {
 thread_local std::string g_err;
 int fail(int code, const std::string &msg) {
   g_err = msg;
   return code;
 }
+} // namespace
+
+int heom::set_error(int code, const std::string &msg) { return fail(code, msg); }
+
+namespace {
 int cuda_fail(cudaError_t e, const char *what) {
   return fail(HEOM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }

@@ -876,10 +876,25 @@ std::string scan_describe(const ScanState &s) {
   return b;
 }
 
+cudaError_t scan_enqueue(const ScanState &s, const heom_scan_point *d_pts, int n, double *d_P,
+                         const long long *d_offsets, cudaStream_t st) {
+  return enqueue(s, d_pts, n, d_P, d_offsets, st);
+}
+
 int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
   if (!s.supported) return 0;
+  std::vector<double> sys;
+  scan_system_host(p, sys);
+  cudaError_t e = cudaMemcpyAsync(s.d_sys, sys.data(), sizeof(double) * sys.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) { s_err = std::string("scan system upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  return 0;
+}
+
+// Packed system of the current sample: Hd[N], Hoff[N x N], X0, X1^T, X2^T, X3.
+void scan_system_host(const heom::Problem &p, std::vector<double> &sys) {
   const int N = p.N(), NN = N * N;
-  std::vector<double> sys(sys_doubles(N), 0.0);
+  sys.assign(sys_doubles(N), 0.0);
   double *Hd = sys.data(), *Hoff = Hd + N, *Xs = Hoff + 2 * NN, *X3 = Xs + 6 * NN;
   for (int i = 0; i < N; i++)
     for (int j = 0; j < N; j++) {
@@ -900,10 +915,6 @@ int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
       X3[2 * t] = p.X[3][2 * t];
       X3[2 * t + 1] = p.X[3][2 * t + 1];
     }
-  cudaError_t e = cudaMemcpyAsync(s.d_sys, sys.data(), sizeof(double) * sys.size(), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) { s_err = std::string("scan system upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
-  return 0;
 }
 
 static int autotune(ScanState &s, const heom::Problem &p, cudaStream_t st) {
@@ -967,7 +978,9 @@ static int autotune(ScanState &s, const heom::Problem &p, cudaStream_t st) {
   return 0;
 }
 
-int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_points, bool tune, cudaStream_t st) {
+// Launch shape, kernel attributes and the packed read-only tables, with no device
+// allocation.  Returns false (s.why set) when the scan kernel cannot hold the problem.
+bool scan_prepare(ScanState &s, const heom::Problem &p, int precision, int max_points, std::vector<unsigned char> &tb) {
   s = ScanState();
   s.precision = precision == HEOM_FP64_EXACT ? HEOM_FP64 : precision;
   s.N = p.N();
@@ -989,7 +1002,7 @@ int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_point
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (s.N > 15 || s.n_ado >= 32768) {
     s.why = "scan kernel supports N <= 15 and fewer than 32768 ADOs";
-    return 0;
+    return false;
   }
   // default shape: the first feasible variant (row-block forms come first)
   s.variant = -1;
@@ -998,7 +1011,7 @@ int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_point
   if (s.variant < 0) {
     s.why = "state does not fit in one CTA's shared memory (" +
             std::to_string(smem_for(s, kVariants[kNumVariants - 1])) + " B)";
-    return 0;
+    return false;
   }
   for (const Variant &v : kVariants)
     if (feasible(s, v, max_smem)) {
@@ -1006,10 +1019,17 @@ int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_point
       cudaFuncSetAttribute(v.f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_for(s, v));
     }
   select_variant(s, s.variant);
+  // HEOM_SCAN_VARIANT=<index into the variant table> pins the launch shape (profiling).
+  if (const char *ev = std::getenv("HEOM_SCAN_VARIANT")) {
+    const int vi = std::atoi(ev);
+    if (vi >= 0 && vi < kNumVariants && feasible(s, kVariants[vi], max_smem)) {
+      select_variant(s, vi);
+      s.pinned = true;
+    }
+  }
   // tables
   TableLayout tl(p.n_ado, p.M, p.K_m);
-  std::vector<unsigned char> tb(tl.total, 0);
-  const size_t nM = (size_t)p.n_ado * p.M;
+  tb.assign(tl.total, 0);
   short *up = (short *)(tb.data() + tl.up), *dn = (short *)(tb.data() + tl.dn);
   double *x = (double *)(tb.data() + tl.x), *y = (double *)(tb.data() + tl.y);
   double *damp = (double *)(tb.data() + tl.damp), *alpha = (double *)(tb.data() + tl.alpha);
@@ -1024,11 +1044,18 @@ int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_point
       x[q] = p.up[q] >= 0 ? std::sqrt((nd + 1.0) * ab) : 0.0;
       y[q] = p.dn[q] >= 0 ? std::sqrt(nd / ab) : 0.0;
     }
-  (void)nM;
   std::memcpy(damp, p.damp.data(), sizeof(double) * 2 * p.n_ado);
   std::memcpy(alpha, p.alpha.data(), sizeof(double) * 2 * p.K_m);
-  cudaError_t e = cudaMalloc(&s.d_tables, tl.total);
-  if (e == cudaSuccess) e = cudaMemcpy(s.d_tables, tb.data(), tl.total, cudaMemcpyHostToDevice);
+  s.tables_bytes = tl.total;
+  s.sys_doubles = sys_doubles(s.N);
+  return true;
+}
+
+int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_points, bool tune, cudaStream_t st) {
+  std::vector<unsigned char> tb;
+  if (!scan_prepare(s, p, precision, max_points, tb)) return 0; // unsupported: s.why says why
+  cudaError_t e = cudaMalloc(&s.d_tables, s.tables_bytes);
+  if (e == cudaSuccess) e = cudaMemcpy(s.d_tables, tb.data(), s.tables_bytes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMalloc(&s.d_sys, sizeof(double) * sys_doubles(s.N));
   if (e == cudaSuccess) e = cudaMalloc(&s.d_pts, sizeof(heom_scan_point) * max_points);
   if (e == cudaSuccess) e = cudaMalloc(&s.d_offsets, sizeof(long long) * max_points);
@@ -1040,15 +1067,7 @@ int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_point
   s.supported = true;
   int rc = scan_upload_system(s, p, st);
   if (rc) return rc;
-  // HEOM_SCAN_VARIANT=<index into the variant table> pins the launch shape (profiling).
-  if (const char *ev = std::getenv("HEOM_SCAN_VARIANT")) {
-    const int vi = std::atoi(ev);
-    if (vi >= 0 && vi < kNumVariants && feasible(s, kVariants[vi], max_smem)) {
-      select_variant(s, vi);
-      return 0;
-    }
-  }
-  if (tune) {
+  if (tune && !s.pinned) {
     // tuning runs with the current (possibly zero) H and X; it only measures time
     rc = autotune(s, p, st);
     if (rc) return rc;

@@ -19,6 +19,7 @@ struct ScanState {
   int variant = 0, ept = 8, threads = 0, grid = 0, sm_count = 0;
   size_t smem = 0;
   float tune_ms = 0;
+  bool pinned = false;           // launch shape fixed by HEOM_SCAN_VARIANT
   // problem constants
   float t_start = 0, dt = 0;
   int stride = 1;
@@ -45,6 +46,14 @@ struct ScanState {
 };
 
 int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_points, bool autotune, cudaStream_t st);
+// Shape + packed tables without any device allocation (false: unsupported, s.why set).
+bool scan_prepare(ScanState &s, const heom::Problem &p, int precision, int max_points,
+                  std::vector<unsigned char> &tables);
+// Packed system matrices of the problem's current sample (s.sys_doubles entries).
+void scan_system_host(const heom::Problem &p, std::vector<double> &sys);
+// Enqueue [order kernel, scan kernel] on st using the device pointers held in s.
+cudaError_t scan_enqueue(const ScanState &s, const heom_scan_point *d_pts, int n, double *d_P,
+                         const long long *d_offsets, cudaStream_t st);
 int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st);
 int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, const long long *offsets,
                   long long total, cudaStream_t st);

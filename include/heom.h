@@ -130,6 +130,22 @@ int heom_run_scan(heom_plan *plan, const heom_scan_point *pts, int n, double *P,
 int heom_run_scan_device(heom_plan *plan, const heom_scan_point *d_pts, int n, double *d_P,
                          const long long *d_offsets);
 
+/* Delay scan that performs no device allocation, for callers that cannot let a library
+ * allocate device memory (a service that reserves its whole budget at start-up in its own
+ * pool or an ML framework's caching allocator, or an application that allows allocation
+ * only during initialisation).  No counterpart in the reference.  Same computation as
+ * heom_run_scan_device with the default launch shape, on the caller's current device and
+ * the given stream (NULL = legacy default stream); inputs and outputs are the caller's
+ * device buffers, the problem comes from the host handle.  Its scratch (work-queue
+ * counter, point ordering, packed tables and system matrices) lives in one 4 MiB
+ * file-scope device array that every GPU loading the library holds until exit: at most
+ * 65536 points per call, and the problem's tables must fit (else HEOM_ERR_CAPACITY).
+ * All calls on a device share that array; calls whose GPU work overlaps race and must be
+ * serialised by the caller.  The first call on a device resolves the array's address;
+ * make it before any stream capture on that device.  Asynchronous: no synchronisation. */
+int heom_run_scan_noalloc(const heom_problem *p, int precision, const heom_scan_point *d_pts, int n,
+                          double *d_P, const long long *d_offsets, void *stream);
+
 /* Launch shape chosen by the autotuner for this plan ("threads/CTA, CTAs/SM"). */
 int heom_plan_describe(const heom_plan *plan, char *buf, int len);
 /* Number of device kernel launches issued by this plan since creation. */
