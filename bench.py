@@ -40,6 +40,10 @@ sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
 METRIC = "2DES propagations/sec, chosen vs plain FP64 on 1 B200 at ≤1e-6 P(t) err"
 UNIT = "propagations/s"
 KEY = os.path.join(ROOT, "tests", "golden", "keys", "c0_dimer.key")
+# dram__bytes_read.sum + dram__bytes_write.sum of the scan kernel from one ncu capture of
+# `bench.py --profile-run fp32-bulk` (418,304 B over 92,768 point-steps), scaled to a full
+# launch by point-steps (inputs, tables and P(t) scale with points and steps).
+DRAM_BYTES_PER_POINT_STEP = 418304.0 / 92768.0
 TEMPLATE = os.path.join(ROOT, "tests", "golden", "keys", "c2_dimer_scan.key-tmpl")
 
 
@@ -327,7 +331,8 @@ def run_ours(a):
                     "d2h_bytes_per_step": int(16 * tot)},
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": DRAM_BYTES_PER_POINT_STEP * sum(steps_of(r[3]) for r in rows),
                          "note": ("algorithmic flops = 3 trajectories x RK4 steps x "
                                   f"{F:.0f} flop/step (4 stages: 16N^3 + 24N^2 per ADO, 16N per link); "
                                   "peak = FP32 FMA throughput measured in this run by the library's "
