@@ -33,8 +33,9 @@ UNITS = [
     ("scan.cu", ["-Xptxas", "-warn-spills"]),
     ("peak.cu", []),
     ("noalloc.cu", []),
+    ("sg.cu", []),
 ]
-HEADERS = ["heom_host.h", "kernels.h", "exact.cuh", "scan.h"]
+HEADERS = ["heom_host.h", "kernels.h", "exact.cuh", "scan.h", "scan_pm.cuh", "sg.cuh"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -17,6 +17,7 @@
 #include "heom_host.h"
 #include "kernels.h"
 #include "scan.h"
+#include "sg.cuh"
 
 namespace {
 thread_local std::string g_err;
@@ -77,13 +78,17 @@ struct heom_plan {
   int chunk = 8;
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   heom_dev::ExactArgs args{};
-  // scan path
+  // scan path (shared-memory resident) and staged path (any size), the latter built on
+  // first use
   heom_dev::ScanState scan;
+  heom_dev::SgState sg;
+  bool sg_ready = false;
   std::string desc;
   ~heom_plan() {
     for (auto &g : graph)
       if (g) cudaGraphExecDestroy(g);
     heom_dev::scan_release(scan);
+    if (sg_ready) heom_dev::sg_release(sg);
     d_H.release(); d_Xs.release(); d_X3.release(); d_damp.release(); d_ops.release(); d_op_start.release();
     d_flags.release(); d_field.release(); d_P.release(); d_work.release(); d_rec.release(); d_base.release();
     d_trajs.release();
@@ -113,7 +118,33 @@ int upload_system(heom_plan *pl) {
   CK(cudaStreamSynchronize(pl->stream));
   int rc = heom_dev::scan_upload_system(pl->scan, p, pl->stream);
   if (rc) return rc;
+  if (pl->sg_ready) {
+    rc = heom_dev::sg_upload_system(pl->sg, p, pl->stream);
+    if (rc) return fail(rc, heom_dev::sg_last_error());
+  }
   return HEOM_OK;
+}
+
+int ensure_sg(heom_plan *pl) {
+  if (pl->sg_ready) return HEOM_OK;
+  int rc = heom_dev::sg_init(pl->sg, pl->prob, pl->precision, pl->stream);
+  if (rc) return fail(rc, heom_dev::sg_last_error());
+  pl->sg_ready = true;
+  return HEOM_OK;
+}
+
+// Staged path: n points of C components (see sg.cuh); P receives `total` points.
+int run_sg(heom_plan *pl, int C, const int mask[3], const heom_scan_point *pts, int n, double *P,
+           const long long *offsets, long long total) {
+  int rc = ensure_sg(pl);
+  if (rc) return rc;
+  rc = heom_dev::sg_run(pl->sg, pl->prob, C, mask, pts, n, P, offsets, total, pl->stream);
+  if (rc) return fail(rc, heom_dev::sg_last_error());
+  return HEOM_OK;
+}
+
+heom_scan_point key_point(const heom::Problem &p) {
+  return heom_scan_point{p.pulses[0].tau0, p.pulses[1].tau0, p.pulses[2].tau0, p.t_end, 0};
 }
 
 // Run up to three trajectories of the exact path concurrently.
@@ -367,6 +398,19 @@ int heom_plan_update(heom_plan *pl, const heom_problem *h) {
 int heom_run_traj(heom_plan *pl, int nv1, int nv2, int nv3, double *P, int cap, int *n_out) {
   if (!pl || !n_out) return fail(HEOM_ERR_ARG, "null argument");
   CK(cudaSetDevice(pl->device));
+  if (pl->precision != HEOM_FP64_EXACT) {
+    const heom_scan_point pt = key_point(pl->prob);
+    const int n = heom::count_records(pl->prob, pt.tau3, pt.t_end);
+    *n_out = n;
+    if (n > cap || (!P && n > 0)) return fail(HEOM_ERR_CAPACITY, "output buffer too small");
+    const int mask[3] = {nv1 == 1, nv2 == 1, nv3 == 1};
+    const long long off = 0;
+    std::vector<double> tmp(2 * (size_t)std::max(n, 1));
+    int rc = run_sg(pl, 1, mask, &pt, 1, tmp.data(), &off, n);
+    if (rc) return rc;
+    if (n) std::memcpy(P, tmp.data(), sizeof(double) * 2 * n);
+    return HEOM_OK;
+  }
   const int m[1][3] = {{nv1, nv2, nv3}};
   std::vector<std::vector<double>> out;
   int rc = run_exact(pl, m, 1, out);
@@ -382,6 +426,25 @@ int heom_run_2des(heom_plan *pl, double *P, double *p_traj, int cap, int *n_out)
   if (!pl || !n_out) return fail(HEOM_ERR_ARG, "null argument");
   CK(cudaSetDevice(pl->device));
   static const int masks[3][3] = {{1, 1, 1}, {1, 1, 0}, {1, 0, 1}}; // CPU_2DES.cpp:65-71
+  if (pl->precision != HEOM_FP64_EXACT) {
+    // combined output in the mixed-difference basis; the three trajectories on request
+    const heom_scan_point pt = key_point(pl->prob);
+    const int n = heom::count_records(pl->prob, pt.tau3, pt.t_end);
+    *n_out = n;
+    if (n > cap || (!P && n > 0)) return fail(HEOM_ERR_CAPACITY, "output buffer too small");
+    const long long off = 0;
+    std::vector<double> tmp(2 * (size_t)std::max(n, 1));
+    int rc = run_sg(pl, 4, nullptr, &pt, 1, tmp.data(), &off, n);
+    if (rc) return rc;
+    if (n) std::memcpy(P, tmp.data(), sizeof(double) * 2 * n);
+    if (p_traj)
+      for (int t = 0; t < 3; t++) {
+        rc = run_sg(pl, 1, masks[t], &pt, 1, tmp.data(), &off, n);
+        if (rc) return rc;
+        if (n) std::memcpy(p_traj + 2 * (size_t)t * cap, tmp.data(), sizeof(double) * 2 * n);
+      }
+    return HEOM_OK;
+  }
   std::vector<std::vector<double>> out;
   int rc = run_exact(pl, masks, 3, out);
   if (rc) return rc;
@@ -414,6 +477,8 @@ int heom_run_scan(heom_plan *pl, const heom_scan_point *pts, int n, double *P, c
   CK(cudaSetDevice(pl->device));
   long long total = 0;
   for (int i = 0; i < n; i++) total = std::max(total, offsets[i] + counts[i]);
+  if (!pl->scan.supported) // hierarchy too large for one CTA: staged path
+    return run_sg(pl, 4, nullptr, pts, n, P, offsets, total);
   int rc = heom_dev::scan_run_host(pl->scan, pts, n, P, offsets, total, pl->stream);
   if (rc) return fail(rc, heom_dev::scan_last_error());
   pl->launches += heom_dev::scan_launches_per_run(pl->scan);
