@@ -100,6 +100,10 @@ def lib() -> ctypes.CDLL:
         "heom_plan_destroy": (None, [P]),
         "heom_measure_fma_peak": (I, [I, I, D]),
         "heom_run_scan_noalloc": (I, [P, I, P, I, P, P, P]),
+        "heom_problem_param_count": (I, [P]),
+        "heom_problem_param_dH": (I, [P, I, D]),
+        "heom_problem_set_bath_scale": (I, [P, I, I, ctypes.c_double]),
+        "heom_adjoint_scan": (I, [P, P, I, ctypes.POINTER(ctypes.c_longlong), ctypes.c_longlong, D, D, D]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -166,6 +170,22 @@ class Problem:
         out = np.zeros((inf.n_ado, inf.K * inf.K_m), dtype=np.uint8)
         _check(lib().heom_problem_get_ado(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte))))
         return out
+
+    # ---- gradient parameters: site energies, couplings (cm^-1), bath amplitude scales
+    def param_count(self) -> int:
+        n = lib().heom_problem_param_count(self._h)
+        if n < 0:
+            _check(n)
+        return n
+
+    def param_dH(self, i: int) -> np.ndarray:
+        N = self.info.sys_size
+        out = np.zeros((N, N), dtype=np.complex128)
+        _check(lib().heom_problem_param_dH(self._h, i, _dptr(out)))
+        return out
+
+    def set_bath_scale(self, site: int, line: int, scale: float) -> None:
+        _check(lib().heom_problem_set_bath_scale(self._h, site, line, float(scale)))
 
 
 @dataclass
@@ -244,6 +264,19 @@ class Plan:
                                    off.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
                                    cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
         return ScanResult(P[:tot], off, cnt)
+
+    def adjoint_scan(self, points: np.ndarray, dLdP: np.ndarray, layout=None):
+        """Forward scan P (FP64, mixed-difference basis) and the gradient of
+        Re sum conj(dLdP) P with respect to the problem's parameters."""
+        pts, off, cnt, tot = layout if layout is not None else self.scan_layout(points)
+        g = np.ascontiguousarray(dLdP, dtype=np.complex128)
+        assert g.shape == (tot,)
+        P = np.zeros(max(tot, 1), dtype=np.complex128)
+        grad = np.zeros(self.problem.param_count(), dtype=np.float64)
+        _check(lib().heom_adjoint_scan(self._h, pts.ctypes.data_as(ctypes.c_void_p), len(pts),
+                                       off.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), tot, _dptr(g),
+                                       _dptr(P), _dptr(grad)))
+        return ScanResult(P[:tot], off, cnt), grad
 
     def run_scan_device(self, d_pts: int, n: int, d_P: int, d_offsets: int) -> None:
         """Device-pointer form (e.g. torch tensors' data_ptr()); asynchronous on the plan's stream."""

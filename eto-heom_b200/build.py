@@ -34,6 +34,7 @@ UNITS = [
     ("peak.cu", []),
     ("noalloc.cu", []),
     ("sg.cu", []),
+    ("adjoint.cu", []),
 ]
 HEADERS = ["heom_host.h", "kernels.h", "exact.cuh", "scan.h", "scan_pm.cuh", "sg.cuh"]
 

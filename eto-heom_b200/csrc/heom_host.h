@@ -47,6 +47,10 @@ struct Problem {
   double angle[4] = {0, 0, 0, 0};
   bool have_polar = false, have_dipole = false, have_bath = false, have_pulse = false;
   std::vector<double> alpha, alpha_t, gamma; // K_m complex (same for every site)
+  // Per (site j, line k) amplitude scale: alpha_jk = bath_scale[j*K_m + k] * alpha_k.  The
+  // reference stores alpha per site (param.h:70); its parser fills identical copies, i.e.
+  // every scale is 1.  The scales are the ETO amplitude parameters of the adjoint.
+  std::vector<double> bath_scale;
   Pulse pulses[3];
   float t_start = 0, t_end = 0, step_size = 0, print_step = 0;
 
@@ -70,6 +74,22 @@ struct Problem {
 
 // Parse; on failure returns false and fills err.  Status code in *code.
 bool parse_key(const std::string &path, int flags, Problem &p, std::string &err, int *code);
+
+// Complex amplitude of line k on site j (alpha_jk).
+void bath_alpha(const Problem &p, int j, int k, double *ar, double *ai);
+// Up/down hierarchy coefficients of ADO n, offset o = j + k K, as the staged and scan
+// kernels tabulate them: x = sqrt((n_o + 1) |alpha_jk|), y = sqrt(n_o / |alpha_jk|) *
+// scale_jk (so that y * alpha_k = sqrt(n_o/|alpha_jk|) alpha_jk).
+double coupling_x(const Problem &p, int n, int o);
+double coupling_y(const Problem &p, int n, int o);
+
+// Gradient parameters: site energies eps_1..eps_{s-1} (cm^-1), couplings J_ab (a < b,
+// row-major, cm^-1), bath amplitude scales (j outer, k inner).
+int n_params(const Problem &p);
+// dH/dtheta_i (N x N complex) for the Hamiltonian parameters (zero for bath scales),
+// through construct_Hal's two-exciton block with the diagonal sort permutation held
+// fixed at the key's order.
+void param_dH(const Problem &p, int i, cbuf &dH);
 // Build ADO list, neighbour tables, damping scalars and coupling ops.
 void build_hierarchy(Problem &p);
 // construct_Hal (draw = true: disorder from the RNG) then orientation (rotate).

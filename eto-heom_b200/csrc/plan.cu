@@ -495,6 +495,41 @@ int heom_run_scan_device(heom_plan *pl, const heom_scan_point *d_pts, int n, dou
   return HEOM_OK;
 }
 
+int heom_problem_param_count(const heom_problem *h) {
+  if (!h) return fail(HEOM_ERR_ARG, "null problem");
+  return heom::n_params(h->p);
+}
+
+int heom_problem_param_dH(const heom_problem *h, int i, double *dH) {
+  if (!h || !dH) return fail(HEOM_ERR_ARG, "null argument");
+  if (i < 0 || i >= heom::n_params(h->p)) return fail(HEOM_ERR_ARG, "parameter index out of range");
+  heom::cbuf D;
+  heom::param_dH(h->p, i, D);
+  std::memcpy(dH, D.data(), sizeof(double) * D.size());
+  return HEOM_OK;
+}
+
+int heom_problem_set_bath_scale(heom_problem *h, int site, int line, double scale) {
+  if (!h) return fail(HEOM_ERR_ARG, "null problem");
+  heom::Problem &p = h->p;
+  if (site < 0 || site >= p.K || line < 0 || line >= p.K_m || !(scale > 0)) return fail(HEOM_ERR_ARG, "bad site/line/scale");
+  p.bath_scale[(size_t)site * p.K_m + line] = scale;
+  heom::build_hierarchy(p);
+  return HEOM_OK;
+}
+
+int heom_adjoint_scan(heom_plan *pl, const heom_scan_point *pts, int n, const long long *offsets, long long total,
+                      const double *dLdP, double *P, double *grad) {
+  if (!pl || (!pts && n > 0) || !offsets || !dLdP || !P || !grad || n < 0 || total < 0)
+    return fail(HEOM_ERR_ARG, "bad argument");
+  CK(cudaSetDevice(pl->device));
+  int rc = heom_dev::adjoint_scan(pl->prob, pts, n, offsets, total, dLdP, P, grad, &pl->launches, pl->stream);
+  if (rc) return fail(rc, heom_dev::adj_last_error());
+  for (long long q = 0; q < 2 * total; q++)
+    if (!std::isfinite(P[q])) return fail(HEOM_ERR_NUMERIC, "non-finite P(t) in the adjoint forward pass");
+  return HEOM_OK;
+}
+
 int heom_plan_describe(const heom_plan *pl, char *buf, int len) {
   if (!pl || !buf || len <= 0) return fail(HEOM_ERR_ARG, "bad argument");
   std::snprintf(buf, (size_t)len, "%s", pl->desc.c_str());

@@ -262,6 +262,7 @@ bool parse_key(const std::string &path, int flags, Problem &p, std::string &err,
   if (p.K < 1 || p.K > p.single_size - 1) return fail("HEOM K must be between 1 and SIZE-1");
   if (p.L < 0 || p.L > 32) return fail("HEOM depth L must be between 0 and 32");
   if (p.K * p.K_m > 255) return fail("K * K_m above 255");
+  p.bath_scale.assign((size_t)p.K * p.K_m, 1.0);
   build_hierarchy(p);
   if (p.n_ado <= 0) return fail("empty hierarchy");
   p.H.assign(2 * (size_t)p.N() * p.N(), 0.0);
@@ -359,7 +360,9 @@ void build_hierarchy(Problem &p) {
         if ((int)a[off] >= L) continue;
         int t = p.up[n * M + off];
         if (t < 0) continue;
-        double x = std::sqrt(((double)a[off] + 1) * std::hypot(p.alpha[2 * k], p.alpha[2 * k + 1]));
+        double ajr, aji;
+        bath_alpha(p, j, k, &ajr, &aji);
+        double x = std::sqrt(((double)a[off] + 1) * std::hypot(ajr, aji));
         // rho+ S_j: coefficient alpha = gsl_complex_mul_real(MINUS_ICNT, x) = (x*0, x*-1).
         const double a1r = x * 0.0, a1i = x * -1.0;
         // S_j rho+: alpha = (x*0, x*1); zgemm first forms temp = alpha * S[s][s].
@@ -374,11 +377,13 @@ void build_hierarchy(Problem &p) {
           if ((int)a[off] <= 0) continue;
           int t = p.dn[n * M + off];
           if (t < 0) continue;
-          double ar = p.alpha[2 * k], ai = p.alpha[2 * k + 1];
+          double ar, ai;
+          bath_alpha(p, j, k, &ar, &ai);
+          const double sc = p.bath_scale.empty() ? 1.0 : p.bath_scale[(size_t)j * Km + k];
           double y = std::sqrt((double)a[off] / std::hypot(ar, ai));
           double ur = y * ar, ui = y * ai;            // gsl_complex_mul_real(alpha, y)
           double x1r = 0.0 * ur - 1.0 * ui, x1i = 0.0 * ui + 1.0 * ur;   // ICNT * (.)
-          double vr = y * p.alpha_t[2 * k], vi = y * p.alpha_t[2 * k + 1];
+          double vr = y * (sc * p.alpha_t[2 * k]), vi = y * (sc * p.alpha_t[2 * k + 1]);
           double x2r = 0.0 * vr - (-1.0) * vi, x2i = 0.0 * vi + (-1.0) * vr; // MINUS_ICNT * (.)
           CouplingOp c1{CouplingOp::kRow, j + 1, t, 0, x1r * 1.0 - x1i * 0.0, x1r * 0.0 + x1i * 1.0};
           CouplingOp c2{CouplingOp::kCol, j + 1, t, 0, x2r, x2i};
@@ -530,6 +535,75 @@ Schedule make_schedule(const Problem &p, const double tau[3], float t_end, const
     t += p.step_size;
   }
   return s;
+}
+
+// ------------------------------------------------------------------ parameters
+void bath_alpha(const Problem &p, int j, int k, double *ar, double *ai) {
+  const double s = p.bath_scale.empty() ? 1.0 : p.bath_scale[(size_t)j * p.K_m + k];
+  *ar = s * p.alpha[2 * k];
+  *ai = s * p.alpha[2 * k + 1];
+}
+
+double coupling_x(const Problem &p, int n, int o) {
+  if (p.up[(size_t)n * p.M + o] < 0) return 0.0;
+  const int j = o % p.K, k = o / p.K;
+  double ar, ai;
+  bath_alpha(p, j, k, &ar, &ai);
+  return std::sqrt((p.ado[(size_t)n * p.M + o] + 1.0) * std::hypot(ar, ai));
+}
+
+double coupling_y(const Problem &p, int n, int o) {
+  if (p.dn[(size_t)n * p.M + o] < 0) return 0.0;
+  const int j = o % p.K, k = o / p.K;
+  double ar, ai;
+  bath_alpha(p, j, k, &ar, &ai);
+  const double s = p.bath_scale.empty() ? 1.0 : p.bath_scale[(size_t)j * p.K_m + k];
+  return std::sqrt(p.ado[(size_t)n * p.M + o] / std::hypot(ar, ai)) * s;
+}
+
+int n_params(const Problem &p) {
+  const int ns = p.single_size - 1;
+  return ns + ns * (ns - 1) / 2 + p.K * p.K_m;
+}
+
+void param_dH(const Problem &p, int i, cbuf &dH) {
+  const int N = p.N(), s = p.single_size, ns = s - 1;
+  dH.assign(2 * (size_t)N * N, 0.0);
+  std::vector<double> D((size_t)s * s, 0.0); // single block, fs^-1 per cm^-1
+  if (i < ns) {
+    // site energy eps_{i+1}: its diagonal lands where construct_Hal's sort puts it
+    // (dynamics.cpp:24-27, index 0 = 0.0 included); the permutation is held fixed.
+    std::vector<std::pair<double, int>> d(s);
+    for (int a = 0; a < s; a++) d[a] = {a == 0 ? 0.0 : re(p.Hkey, N, a, a), a};
+    std::stable_sort(d.begin(), d.end(), [](const std::pair<double, int> &x, const std::pair<double, int> &y) {
+      return x.first < y.first;
+    });
+    for (int pos = 1; pos < s; pos++)
+      if (d[pos].second == i + 1) D[(size_t)pos * s + pos] = 1.0 / kHbar;
+  } else if (i < ns + ns * (ns - 1) / 2) {
+    int q = i - ns;
+    for (int a = 1; a < s; a++)
+      for (int b = a + 1; b < s; b++, q--)
+        if (q == 0) D[(size_t)a * s + b] = D[(size_t)b * s + a] = 1.0 / kHbar;
+  } else {
+    return; // bath scale: H does not depend on it
+  }
+  for (int a = 0; a < s; a++)
+    for (int b = 0; b < s; b++) re(dH, N, a, b) = D[(size_t)a * s + b];
+  if (p.single_manifold) return;
+  // two-exciton block, linear in the single block (dynamics.cpp:29-49)
+  for (int x = s; x < N; x++)
+    for (int y = s; y < N; y++) {
+      const int a = p.d_a[x], b = p.d_b[x], c = p.d_a[y], d = p.d_b[y];
+      double v;
+      if (x == y) {
+        v = D[(size_t)a * s + a] + D[(size_t)b * s + b];
+      } else {
+        v = (a == c) * (1 - (b == d)) * D[(size_t)b * s + d] + (a == d) * (1 - (b == c)) * D[(size_t)b * s + c] +
+            (b == c) * (1 - (a == d)) * D[(size_t)a * s + d] + (b == d) * (1 - (a == c)) * D[(size_t)a * s + c];
+      }
+      re(dH, N, x, y) = v;
+    }
 }
 
 int count_records(const Problem &p, double tau3, float t_end) {

@@ -1036,13 +1036,10 @@ bool scan_prepare(ScanState &s, const heom::Problem &p, int precision, int max_p
   for (int n = 0; n < p.n_ado; n++)
     for (int o = 0; o < p.M; o++) {
       const size_t q = (size_t)n * p.M + o;
-      const int k = o / p.K;
-      const double ab = std::hypot(p.alpha[2 * k], p.alpha[2 * k + 1]);
-      const int nd = p.ado[q];
       up[q] = (short)p.up[q];
       dn[q] = (short)p.dn[q];
-      x[q] = p.up[q] >= 0 ? std::sqrt((nd + 1.0) * ab) : 0.0;
-      y[q] = p.dn[q] >= 0 ? std::sqrt(nd / ab) : 0.0;
+      x[q] = heom::coupling_x(p, n, o);
+      y[q] = heom::coupling_y(p, n, o);
     }
   std::memcpy(damp, p.damp.data(), sizeof(double) * 2 * p.n_ado);
   std::memcpy(alpha, p.alpha.data(), sizeof(double) * 2 * p.K_m);

@@ -288,13 +288,11 @@ int sg_init(SgState &s, const heom::Problem &p, int precision, cudaStream_t st) 
   double *xc = (double *)(tb.data() + tl.xc), *yc = (double *)(tb.data() + tl.yc);
   int *up = (int *)(tb.data() + tl.up), *dn = (int *)(tb.data() + tl.dn);
   for (size_t q = 0; q < nM; q++) {
-    const int k = (int)(q % p.M) / p.K;
-    const double ab = std::hypot(p.alpha[2 * k], p.alpha[2 * k + 1]);
-    const int nd = p.ado[q];
+    const int n = (int)(q / p.M), o = (int)(q % p.M);
     up[q] = p.up[q];
     dn[q] = p.dn[q];
-    xc[q] = p.up[q] >= 0 ? std::sqrt((nd + 1.0) * ab) : 0.0;
-    yc[q] = p.dn[q] >= 0 ? std::sqrt(nd / ab) : 0.0;
+    xc[q] = heom::coupling_x(p, n, o);
+    yc[q] = heom::coupling_y(p, n, o);
   }
   std::memcpy(tb.data() + tl.damp, p.damp.data(), sizeof(double) * 2 * p.n_ado);
   std::memcpy(tb.data() + tl.alpha, p.alpha.data(), sizeof(double) * 2 * p.K_m);

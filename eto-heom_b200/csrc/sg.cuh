@@ -53,4 +53,10 @@ int sg_run(SgState &s, const heom::Problem &p, int C, const int mask[3], const h
 void sg_release(SgState &s);
 const char *sg_last_error();
 
+// Adjoint of a delay scan (adjoint.cu): forward readout into P_host and the gradient of
+// Re sum_i conj(g_i) P_i with respect to heom::n_params(p) parameters into grad.
+int adjoint_scan(const heom::Problem &p, const heom_scan_point *pts, int n, const long long *offsets, long long total,
+                 const double *g_host, double *P_host, double *grad, long long *launches, cudaStream_t st);
+const char *adj_last_error();
+
 } // namespace heom_dev

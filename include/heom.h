@@ -146,6 +146,27 @@ int heom_run_scan_device(heom_plan *plan, const heom_scan_point *d_pts, int n, d
 int heom_run_scan_noalloc(const heom_problem *p, int precision, const heom_scan_point *d_pts, int n,
                           double *d_P, const long long *d_offsets, void *stream);
 
+/* Gradient parameters of a problem, in this order: the site energies eps_1..eps_{s-1}
+ * (cm^-1, HAMILTONIAN diagonal), the couplings J_ab for a < b (cm^-1, row-major), and the
+ * bath amplitude scales s_jk (site j < K outer, line k < K_m inner; alpha_jk = s_jk alpha_k,
+ * 1 as parsed -- the reference keeps alpha per site, param.h:70).  No counterpart in the
+ * reference, which has no gradients. */
+int heom_problem_param_count(const heom_problem *p);
+/* dH/dtheta_i (N x N complex, fs^-1 per cm^-1) through construct_Hal's two-exciton block,
+ * the diagonal sort held at the key's order; zero for bath scales. */
+int heom_problem_param_dH(const heom_problem *p, int i, double *dH);
+/* Set s_jk; plans created afterwards use it. */
+int heom_problem_set_bath_scale(heom_problem *p, int site, int line, double scale);
+
+/* Adjoint gradient of a delay scan (config-4 style fitting).  Runs the scan forward in FP64
+ * (mixed-difference basis, P = p111 - p110 - p101 into P, layout of heom_scan_layout) and
+ * the discrete adjoint of its RK4 steps backwards with checkpoints every ceil(sqrt(steps))
+ * steps, and returns grad_i = d/dtheta_i Re sum_t conj(dLdP_t) P_t for the parameters of
+ * heom_problem_param_count (dLdP: complex gradient of a real objective with respect to each
+ * recorded P).  No counterpart in the reference. */
+int heom_adjoint_scan(heom_plan *plan, const heom_scan_point *pts, int n, const long long *offsets,
+                      long long total, const double *dLdP, double *P, double *grad);
+
 /* Launch shape chosen by the autotuner for this plan ("threads/CTA, CTAs/SM"). */
 int heom_plan_describe(const heom_plan *plan, char *buf, int len);
 /* Number of device kernel launches issued by this plan since creation. */
