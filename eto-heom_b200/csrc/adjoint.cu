@@ -411,14 +411,14 @@ int adjoint_scan(const heom::Problem &p, const heom_scan_point *pts, int n, cons
   const size_t o_rec = a256(o_fl + NS), o_field = a256(o_rec + 4 * NS), o_ns = a256(o_field + 48 * NS);
   const size_t o_off = a256(o_ns + 4 * (size_t)n), o_g = a256(o_off + 8 * (size_t)n), o_P = a256(o_g + 16 * (size_t)total);
   const size_t o_st = a256(o_P + 16 * (size_t)total);
-  const int nbuf = 10 + 2 * nck; // rho_a, rho_b, w1, w2, w3, lam, acc, u_a, u_b, spare, ckpt[nck], seg[nck]
+  const int nbuf = 10 + nck + Kc; // rho_a, rho_b, w1, w2, w3, lam, acc, u_a, u_b, spare, ckpt[nck], seg[Kc]
   const size_t bytes = o_st + SB * (size_t)nbuf;
   const int apc = std::max(1, 256 / NN) * NN > 1024 ? 1 : std::max(1, 256 / NN);
   const int threads = std::min(1024, ((apc * NN + 31) / 32) * 32);
   const size_t smem_f = 16 * 6 * (size_t)NN, smem_b = 16 * 7 * (size_t)NN + 8 * (size_t)M + 16;
   const dim3 grid((nado + apc - 1) / apc, 4, n);
   double2 *rho_a, *rho_b, *w1, *w2, *w3, *lam, *acc, *ua, *ub;
-  std::vector<double2 *> ck(nck), seg(nck);
+  std::vector<double2 *> ck(nck), seg(Kc);
   std::vector<double> gMh((size_t)n * NN * 2), gBh((size_t)n * M);
   long long nl = 0;
   const double h = (double)p.step_size;
@@ -465,10 +465,8 @@ int adjoint_scan(const heom::Problem &p, const heom_scan_point *pts, int n, cons
     for (int b = 0; b < 10; b++) bufs[b] = (double2 *)(dev + o_st + SB * b);
     rho_a = bufs[0]; rho_b = bufs[1]; w1 = bufs[2]; w2 = bufs[3]; w3 = bufs[4];
     lam = bufs[5]; acc = bufs[6]; ua = bufs[7]; ub = bufs[8];
-    for (int k = 0; k < nck; k++) {
-      ck[k] = (double2 *)(dev + o_st + SB * (10 + k));
-      seg[k] = (double2 *)(dev + o_st + SB * (10 + nck + k));
-    }
+    for (int k = 0; k < nck; k++) ck[k] = (double2 *)(dev + o_st + SB * (10 + k));
+    for (int k = 0; k < Kc; k++) seg[k] = (double2 *)(dev + o_st + SB * (10 + nck + k));
   }
   // ---- forward with checkpoints
   adj_init<<<1024, 256, 0, st>>>(rho_a, E, E_pt);
