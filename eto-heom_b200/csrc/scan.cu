@@ -57,7 +57,7 @@ template <> struct V2<float> { using t = float2; };
 template <> struct V2<double> { using t = double2; };
 
 struct ScanArgs {
-  int N, n_ado, M, K, K_m, E, n_points, stride, use_order;
+  int N, n_ado, M, K, K_m, E, n_points, stride, use_order, wcap, ado0;
   float t_start, dt;
   double E0[3], taup[3], w0[3], h;
   const unsigned char *tables;
@@ -70,9 +70,16 @@ struct ScanArgs {
 };
 
 // Table layout (bytes, 16-aligned sections): up int16[nM], dn int16[nM],
-// x double[nM], y double[nM], damp double2[n_ado], alpha double2[K_m].
+// x double[nM], y double[nM], damp double2[n_ado], alpha double2[K_m] (ADOs in the
+// hierarchy's order), then the whole-ADO form's tables with the ADOs in its own order
+// (see scan_pm.cuh): plink PmLinkHost[M][n_ado], pdamp double2[n_ado].
+struct PmLinkHost {
+  double x, by, ay; // up coefficient; down coefficients y*Im(alpha_k), y*Re(alpha_k)
+  int ud;           // up-neighbour | down-neighbour << 16 (0xffff: none), in pm order
+  int pad;
+};
 struct TableLayout {
-  size_t up, dn, x, y, damp, alpha, total;
+  size_t up, dn, x, y, damp, alpha, plink, pdamp, total;
   __host__ __device__ static size_t al(size_t v) { return (v + 15) & ~(size_t)15; }
   __host__ __device__ TableLayout(int n_ado, int M, int K_m) {
     const size_t nM = (size_t)n_ado * M;
@@ -82,7 +89,9 @@ struct TableLayout {
     y = al(x + 8 * nM);
     damp = al(y + 8 * nM);
     alpha = al(damp + 16 * (size_t)n_ado);
-    total = al(alpha + 16 * (size_t)K_m);
+    plink = al(alpha + 16 * (size_t)K_m);
+    pdamp = al(plink + sizeof(PmLinkHost) * nM);
+    total = al(pdamp + 16 * (size_t)n_ado);
   }
 };
 
@@ -763,9 +772,6 @@ struct Variant {
 
 const Variant kVariants[] = {
     {kAdo, 4, 4, 320, scan_pm<float, 4, 4, 320>, scan_pm<double, 4, 4, 320>},
-    {kAdo, 4, 2, 576, scan_pm<float, 4, 2, 576>, scan_pm<double, 4, 2, 576>},
-    {kAdo, 4, 2, 768, scan_pm<float, 4, 2, 768>, scan_pm<double, 4, 2, 768>},
-    {kAdo, 4, 1, 1024, scan_pm<float, 4, 1, 1024>, scan_pm<double, 4, 1, 1024>},
     {kRows, 4, 1, 1024, scan_rows<float, 4, 1, 1024>, scan_rows<double, 4, 1, 1024>},
     {kRows, 4, 2, 640, scan_rows<float, 4, 2, 640>, scan_rows<double, 4, 2, 640>},
     {kRows, 4, 4, 320, scan_rows<float, 4, 4, 320>, scan_rows<double, 4, 4, 320>},
@@ -788,7 +794,7 @@ int threads_for(const ScanState &s, const Variant &v) {
 
 size_t smem_for(const ScanState &s, const Variant &v) {
   const size_t tsz = s.precision == HEOM_FP64 ? 8 : 4;
-  if (v.form == kAdo && v.nt == 4) return pm_smem_bytes<4>(tsz, s.n_ado, s.M, s.K_m, s.E);
+  if (v.form == kAdo && v.nt == 4) return pm_smem_bytes<4>(tsz, s.n_ado, s.M, s.wcap);
   if (v.form == kRows && v.nt == 4) return rows_smem_bytes<4>(tsz, s.n_ado, s.M, s.K_m, s.E);
   return tsz == 8 ? scan_smem_bytes<double>(s.N, s.n_ado, s.M, s.K_m, s.E)
                   : scan_smem_bytes<float>(s.N, s.n_ado, s.M, s.K_m, s.E);
@@ -826,6 +832,8 @@ ScanArgs make_args(const ScanState &s, const heom_scan_point *pts, int n, double
   a.n_points = n;
   a.stride = s.stride;
   a.use_order = use_order;
+  a.wcap = s.wcap;
+  a.ado0 = s.ado0;
   a.t_start = s.t_start;
   a.dt = s.dt;
   for (int q = 0; q < 3; q++) { a.E0[q] = s.E0[q]; a.taup[q] = s.taup[q]; a.w0[q] = s.w0[q]; }
@@ -1004,6 +1012,11 @@ bool scan_prepare(ScanState &s, const heom::Problem &p, int precision, int max_p
     s.why = "scan kernel supports N <= 15 and fewer than 32768 ADOs";
     return false;
   }
+  // pulse-field window tables of the whole-ADO form: dropped (fields evaluated in the
+  // step) if they would not fit beside the state
+  s.wcap = pm_window_cap(s.taup, s.dt);
+  if (pm_smem_bytes<4>(s.precision == HEOM_FP64 ? 8 : 4, s.n_ado, s.M, s.wcap) + 1024 > (size_t)max_smem)
+    s.wcap = 0;
   // default shape: the first feasible variant (row-block forms come first)
   s.variant = -1;
   for (int vi = 0; vi < kNumVariants && s.variant < 0; vi++)
@@ -1043,6 +1056,44 @@ bool scan_prepare(ScanState &s, const heom::Problem &p, int precision, int max_p
     }
   std::memcpy(damp, p.damp.data(), sizeof(double) * 2 * p.n_ado);
   std::memcpy(alpha, p.alpha.data(), sizeof(double) * 2 * p.K_m);
+  // Whole-ADO form: ADOs ordered by depth, deepest first (the deepest tier has no
+  // up-neighbours), then by the pattern of nonzero digits (which down-neighbours exist),
+  // so that the threads of a warp mostly take the same neighbour branches.
+  std::vector<int> perm(p.n_ado), inv(p.n_ado);
+  for (int n = 0; n < p.n_ado; n++) perm[n] = n;
+  auto nzmask = [&](int n) {
+    unsigned m = 0;
+    for (int o = 0; o < p.M; o++)
+      if (p.ado[(size_t)n * p.M + o]) m |= 1u << (o & 31);
+    return m;
+  };
+  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
+    if (p.depth[a] != p.depth[b]) return p.depth[a] > p.depth[b];
+    return nzmask(a) < nzmask(b);
+  });
+  for (int i = 0; i < p.n_ado; i++) inv[perm[i]] = i;
+  s.ado0 = inv[0];
+  PmLinkHost *pl = (PmLinkHost *)(tb.data() + tl.plink);
+  double *pdamp = (double *)(tb.data() + tl.pdamp);
+  for (int n = 0; n < p.n_ado; n++) {
+    const int np = inv[n];
+    pdamp[2 * np] = p.damp[2 * n];
+    pdamp[2 * np + 1] = p.damp[2 * n + 1];
+    for (int o = 0; o < p.M; o++) {
+      const size_t q = (size_t)n * p.M + o;
+      const int k = o / p.K;
+      const double y = heom::coupling_y(p, n, o);
+      PmLinkHost &L = pl[(size_t)o * p.n_ado + np];
+      // a missing link gets zero coefficients (the kernel may read the zero block for it)
+      L.x = p.up[q] >= 0 ? heom::coupling_x(p, n, o) : 0.0;
+      L.by = p.dn[q] >= 0 ? p.alpha[2 * k + 1] * y : 0.0;
+      L.ay = p.dn[q] >= 0 ? p.alpha[2 * k] * y : 0.0;
+      const unsigned u = p.up[q] >= 0 ? (unsigned)inv[p.up[q]] : 0xffffu;
+      const unsigned d = p.dn[q] >= 0 ? (unsigned)inv[p.dn[q]] : 0xffffu;
+      L.ud = (int)(u | (d << 16));
+      L.pad = 0;
+    }
+  }
   s.tables_bytes = tl.total;
   s.sys_doubles = sys_doubles(s.N);
   return true;

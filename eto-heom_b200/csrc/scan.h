@@ -17,6 +17,8 @@ struct ScanState {
   std::string why;
   // launch shape (autotuned)
   int variant = 0, ept = 8, threads = 0, grid = 0, sm_count = 0;
+  int wcap = 0;                  // pulse-field window table length (whole-ADO form)
+  int ado0 = 0;                  // index of ADO 0 in the whole-ADO form's order
   size_t smem = 0;
   float tune_ms = 0;
   bool pinned = false;           // launch shape fixed by HEOM_SCAN_VARIANT
