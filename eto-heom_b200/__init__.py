@@ -10,6 +10,9 @@ param.h:38-82) over the C ABI declared in include/heom.h:
     P, trajs = plan.run_2des()                 # CPU_2DES's p111 - p110 - p101
     P = plan.run_scan(points)                  # a whole delay scan in one launch
 
+    prob = Problem.from_key("population.key", dynamics=True)   # param::param_dynamics
+    pops = Plan(prob, "fp64-exact").run_populations((1, 2))    # dynamics_solver
+
 There is no CPU fallback: every propagation runs in the CUDA kernels of libheom.so,
 and constructing a Plan without a CUDA device raises HeomError.  The package
 directory name contains a hyphen, so load it by path (see load_package()).
@@ -29,6 +32,7 @@ FP64_EXACT, FP64, FP32_BULK = 0, 1, 2
 PRECISIONS = {"fp64-exact": FP64_EXACT, "fp64": FP64, "fp32-bulk": FP32_BULK}
 MAT_H, MAT_X0, MAT_X1, MAT_X2, MAT_X3, MAT_HKEY = range(6)
 KEY_SINGLE_MANIFOLD = 1
+KEY_DYNAMICS = 2
 
 ERRORS = {-1: "argument", -2: "io", -3: "parse", -4: "cuda", -5: "nomem", -6: "capacity",
           -7: "unsupported", -8: "numeric", -9: "timeout"}
@@ -81,6 +85,7 @@ def lib() -> ctypes.CDLL:
         "heom_problem_from_key": (I, [ctypes.c_char_p, I, ctypes.POINTER(P)]),
         "heom_problem_info_get": (I, [P, ctypes.POINTER(ProblemInfo)]),
         "heom_problem_prepare_sample": (I, [P]),
+        "heom_problem_scan_compatible": (I, [P, P]),
         "heom_problem_prepare_identity": (I, [P]),
         "heom_problem_reset_rng": (I, [P]),
         "heom_problem_get_matrix": (I, [P, I, D]),
@@ -91,6 +96,7 @@ def lib() -> ctypes.CDLL:
         "heom_plan_update": (I, [P, P]),
         "heom_run_traj": (I, [P, I, I, I, D, I, ctypes.POINTER(I)]),
         "heom_run_2des": (I, [P, D, D, I, ctypes.POINTER(I)]),
+        "heom_run_populations": (I, [P, ctypes.POINTER(I), I, D, I, ctypes.POINTER(I)]),
         "heom_scan_layout": (I, [P, P, I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(I),
                                  ctypes.POINTER(ctypes.c_longlong)]),
         "heom_run_scan": (I, [P, P, I, D, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(I)]),
@@ -129,10 +135,12 @@ class Problem:
         self._h = handle
 
     @classmethod
-    def from_key(cls, path: str, single_manifold: bool = False) -> "Problem":
+    def from_key(cls, path: str, single_manifold: bool = False, dynamics: bool = False) -> "Problem":
+        """Parse a 2DES key file (param::param_2des) or, with dynamics=True, a
+        population-dynamics key file (param::param_dynamics)."""
         h = ctypes.c_void_p()
-        _check(lib().heom_problem_from_key(os.fsencode(path), KEY_SINGLE_MANIFOLD if single_manifold else 0,
-                                           ctypes.byref(h)))
+        flags = (KEY_SINGLE_MANIFOLD if single_manifold else 0) | (KEY_DYNAMICS if dynamics else 0)
+        _check(lib().heom_problem_from_key(os.fsencode(path), flags, ctypes.byref(h)))
         return cls(h)
 
     def __del__(self):
@@ -151,6 +159,13 @@ class Problem:
 
     def prepare_identity(self) -> None:
         _check(lib().heom_problem_prepare_identity(self._h))
+
+    def scan_compatible(self, other: "Problem") -> bool:
+        """True if the two key files differ at most in pulse times and end time."""
+        rc = lib().heom_problem_scan_compatible(self._h, other._h)
+        if rc < 0:
+            _check(rc)
+        return rc == 1
 
     def reset_rng(self) -> None:
         _check(lib().heom_problem_reset_rng(self._h))
@@ -237,6 +252,17 @@ class Plan:
         n = ctypes.c_int()
         _check(lib().heom_run_traj(self._h, nv1, nv2, nv3, _dptr(out), cap, ctypes.byref(n)))
         return out[:n.value]
+
+    def run_populations(self, sites=(1, 2)) -> np.ndarray:
+        """Populations Re rho_0[s-1][s-1] of the given 1-based sites, every print_step from
+        t_start, with site 1 initially excited (dynamics_solver, dynamics.cpp:202-295)."""
+        s = np.ascontiguousarray(sites, dtype=np.int32)
+        cap = max(self.problem.info.n_record, 1)
+        out = np.zeros((len(s), cap), dtype=np.float64)
+        n = ctypes.c_int()
+        _check(lib().heom_run_populations(self._h, s.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(s),
+                                          _dptr(out), cap, ctypes.byref(n)))
+        return out[:, :n.value]
 
     def run_2des(self):
         cap = max(self.problem.info.n_record, 1)

@@ -1,4 +1,4 @@
-"""Build libheom.so (C ABI + sm_100a kernels) and the heom_2des CLI in-tree.
+"""Build libheom.so (C ABI + sm_100a kernels) and the heom_2des / heom_scan / heom_dynamics CLIs in-tree.
 
     python eto-heom_b200/build.py [--force]
 
@@ -19,7 +19,9 @@ ROOT = os.path.dirname(PKG)
 SRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libheom.so")
-CLI = os.path.join(PKG, "heom_2des")
+CLIS = [(os.path.join(SRC, "heom_2des.cpp"), os.path.join(PKG, "heom_2des")),
+        (os.path.join(SRC, "heom_scan.cpp"), os.path.join(PKG, "heom_scan")),
+        (os.path.join(SRC, "heom_dynamics.cpp"), os.path.join(PKG, "heom_dynamics"))]
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -66,10 +68,10 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
             _run([NVCC, *ARCH, *COMMON, *flags, "-c", src, "-o", obj])
     if force or _newer(LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
-    cli_src = os.path.join(SRC, "heom_2des.cpp")
-    if os.path.exists(cli_src) and (force or _newer(CLI, [cli_src, LIB])):
-        _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include"), cli_src,
-              "-o", CLI, "-L" + PKG, "-lheom", "-Wl,-rpath,$ORIGIN"])
+    for cli_src, cli in CLIS:
+        if force or _newer(cli, [cli_src, LIB, os.path.join(ROOT, "include", "heom.h")]):
+            _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-Wall", "-I" + os.path.join(ROOT, "include"),
+                  cli_src, "-o", cli, "-L" + PKG, "-lheom", "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 

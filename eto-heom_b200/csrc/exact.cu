@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(512) exact_traj_smem(ExactArgs a, const ExactT
     __syncthreads();
     const int rec = tj.rec_idx[i];
     if (rec >= 0) {
-      for (int j = tid; j < N; j += bs) Pt[j] = trace_row_exact(A, a.X3, N, j);
+      for (int j = tid; j < N; j += bs) Pt[j] = trace_row_exact(A, tj.X3 ? tj.X3 : a.X3, N, j);
       __syncthreads();
       if (tid == 0) {
         double tr = 0.0, ti = 0.0;
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(256) exact_stage(ExactArgs a, const ExactTraj 
   if (stage == 1 && n == 0) {
     const int rec = tj.rec_idx[i];
     if (rec >= 0) {
-      for (int j = tid; j < N; j += bs) Pt[j] = trace_row_exact(own, a.X3, N, j);
+      for (int j = tid; j < N; j += bs) Pt[j] = trace_row_exact(own, tj.X3 ? tj.X3 : a.X3, N, j);
       __syncthreads();
       if (tid == 0) {
         double tr = 0.0, ti = 0.0;

@@ -42,6 +42,11 @@ struct Problem {
   int single_size = 0, sys_size = 0, K = 0, K_m = 0, L = 0, n_sample = 0;
   unsigned long seed = 0;
   bool single_manifold = false;
+  // Population-dynamics key (param_dynamics): every level is a site and site j's
+  // coupling operator S_j = |j><j|; 2DES keys put the ground state at level 0 and
+  // S_j = |j+1><j+1|.  level0 is the level of site 1's S (0 or 1).
+  bool dynamics = false;
+  int level0 = 1;
   std::vector<int> d_a, d_b;    // two-exciton level -> (a, b) (param.cpp:127-135)
   cbuf Hkey, Dis, Xx, Xy, Xz;   // N x N
   double angle[4] = {0, 0, 0, 0};

@@ -28,6 +28,7 @@ struct ExactTraj {
   double2 *P;            // recorded points
   double2 *work;         // staged form: A, B, k1, k2, k3 (5 x n_ado x N x N)
   double2 *final_state;  // optional copy of the final state (n_ado x N x N)
+  const double2 *X3;     // readout operator of this trajectory (nullptr: ExactArgs::X3)
   int n_steps, pad;
 };
 

@@ -67,6 +67,7 @@ extern "C" int heom_run_scan_noalloc(const heom_problem *prob, int precision, co
                                      double *d_P, const long long *d_offsets, void *stream) {
   if (!prob || n < 0 || (n > 0 && (!d_pts || !d_P || !d_offsets)))
     return heom::set_error(HEOM_ERR_ARG, "bad argument");
+  if (prob->p.dynamics) return heom::set_error(HEOM_ERR_UNSUPPORTED, "population-dynamics keys have no delay scan");
   if (precision != HEOM_FP32_BULK && precision != HEOM_FP64)
     return heom::set_error(HEOM_ERR_ARG, "heom_run_scan_noalloc takes HEOM_FP32_BULK or HEOM_FP64");
   if (n > kNoAllocMaxPoints)

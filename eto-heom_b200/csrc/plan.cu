@@ -74,9 +74,11 @@ struct heom_plan {
   DevBuf<double2> d_field, d_P, d_work;
   DevBuf<int> d_rec, d_base;
   DevBuf<heom_dev::ExactTraj> d_trajs;
+  DevBuf<double2> d_X3pop; // per-site readout operators of heom_run_populations
   bool use_smem = true;
   int chunk = 8;
-  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+  static constexpr int kMaxTraj = 64; // concurrent exact-path trajectories per launch
+  cudaGraphExec_t graph[kMaxTraj + 1] = {};
   heom_dev::ExactArgs args{};
   // scan path (shared-memory resident) and staged path (any size), the latter built on
   // first use
@@ -91,7 +93,7 @@ struct heom_plan {
     if (sg_ready) heom_dev::sg_release(sg);
     d_H.release(); d_Xs.release(); d_X3.release(); d_damp.release(); d_ops.release(); d_op_start.release();
     d_flags.release(); d_field.release(); d_P.release(); d_work.release(); d_rec.release(); d_base.release();
-    d_trajs.release();
+    d_trajs.release(); d_X3pop.release();
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
 };
@@ -147,10 +149,15 @@ heom_scan_point key_point(const heom::Problem &p) {
   return heom_scan_point{p.pulses[0].tau0, p.pulses[1].tau0, p.pulses[2].tau0, p.t_end, 0};
 }
 
-// Run up to three trajectories of the exact path concurrently.
-int run_exact(heom_plan *pl, const int (*masks)[3], int n_traj, std::vector<std::vector<double>> &out) {
+// Run up to kMaxTraj trajectories of the exact path concurrently (one CTA or block row
+// each).  tau_in: pulse times (nullptr: the key's); X3s: per-trajectory device readout
+// operators (nullptr: the problem's X3).
+int run_exact(heom_plan *pl, const int (*masks)[3], int n_traj, std::vector<std::vector<double>> &out,
+              const double *tau_in = nullptr, const double2 *const *X3s = nullptr) {
   const heom::Problem &p = pl->prob;
-  const double tau[3] = {p.pulses[0].tau0, p.pulses[1].tau0, p.pulses[2].tau0};
+  if (n_traj < 1 || n_traj > heom_plan::kMaxTraj) return fail(HEOM_ERR_ARG, "trajectory count out of range");
+  const double tau[3] = {tau_in ? tau_in[0] : p.pulses[0].tau0, tau_in ? tau_in[1] : p.pulses[1].tau0,
+                         tau_in ? tau_in[2] : p.pulses[2].tau0};
   std::vector<heom::Schedule> sch;
   for (int t = 0; t < n_traj; t++) sch.push_back(heom::make_schedule(p, tau, p.t_end, masks[t]));
   const int ns = sch[0].n_steps, nrec = sch[0].n_record;
@@ -159,7 +166,7 @@ int run_exact(heom_plan *pl, const int (*masks)[3], int n_traj, std::vector<std:
   CK(pl->d_field.ensure((size_t)n_traj * 3 * ns));
   CK(pl->d_rec.ensure((size_t)n_traj * ns));
   CK(pl->d_P.ensure((size_t)n_traj * std::max(nrec, 1)));
-  CK(pl->d_trajs.ensure(3));
+  CK(pl->d_trajs.ensure(n_traj));
   if (!pl->use_smem) CK(pl->d_work.ensure((size_t)n_traj * 5 * tot));
   std::vector<heom_dev::ExactTraj> tr(n_traj);
   for (int t = 0; t < n_traj; t++) {
@@ -174,6 +181,7 @@ int run_exact(heom_plan *pl, const int (*masks)[3], int n_traj, std::vector<std:
     tr[t].P = pl->d_P.ptr + (size_t)t * std::max(nrec, 1);
     tr[t].work = pl->use_smem ? nullptr : pl->d_work.ptr + (size_t)t * 5 * tot;
     tr[t].final_state = nullptr;
+    tr[t].X3 = X3s ? X3s[t] : nullptr;
     tr[t].n_steps = ns;
   }
   CK(cudaMemcpyAsync(pl->d_trajs.ptr, tr.data(), sizeof(heom_dev::ExactTraj) * n_traj, cudaMemcpyHostToDevice,
@@ -255,7 +263,7 @@ int heom_problem_info_get(const heom_problem *h, heom_problem_info *info) {
   info->seed = p.seed;
   info->n_steps = p.n_steps();
   info->print_stride = p.print_stride();
-  info->n_record = heom::count_records(p, p.pulses[2].tau0, p.t_end);
+  info->n_record = heom::count_records(p, p.dynamics ? -HUGE_VAL : p.pulses[2].tau0, p.t_end);
   info->t_start = p.t_start;
   info->t_end = p.t_end;
   info->step_size = p.step_size;
@@ -267,6 +275,23 @@ int heom_problem_info_get(const heom_problem *h, heom_problem_info *info) {
     info->w0[q] = p.pulses[q].w0;
   }
   return HEOM_OK;
+}
+
+int heom_problem_scan_compatible(const heom_problem *a, const heom_problem *b) {
+  if (!a || !b) return fail(HEOM_ERR_ARG, "null problem");
+  const heom::Problem &x = a->p, &y = b->p;
+  bool same = x.single_size == y.single_size && x.sys_size == y.sys_size && x.K == y.K && x.K_m == y.K_m &&
+              x.L == y.L && x.n_sample == y.n_sample && x.seed == y.seed && x.single_manifold == y.single_manifold &&
+              x.d_a == y.d_a && x.d_b == y.d_b && x.Hkey == y.Hkey && x.Dis == y.Dis && x.Xx == y.Xx &&
+              x.Xy == y.Xy && x.Xz == y.Xz && x.have_polar == y.have_polar && x.have_dipole == y.have_dipole &&
+              x.have_bath == y.have_bath && x.have_pulse == y.have_pulse && x.alpha == y.alpha &&
+              x.alpha_t == y.alpha_t && x.gamma == y.gamma && x.bath_scale == y.bath_scale &&
+              x.t_start == y.t_start && x.step_size == y.step_size && x.print_step == y.print_step;
+  for (int q = 0; q < 4; q++) same = same && x.angle[q] == y.angle[q];
+  for (int q = 0; q < 3; q++)
+    same = same && x.pulses[q].E0 == y.pulses[q].E0 && x.pulses[q].taup == y.pulses[q].taup &&
+           x.pulses[q].w0 == y.pulses[q].w0;
+  return same ? 1 : 0;
 }
 
 int heom_problem_prepare_sample(heom_problem *h) {
@@ -324,6 +349,8 @@ int heom_plan_create(const heom_problem *h, const heom_opts *opts, heom_plan **o
   heom_opts o{};
   if (opts) o = *opts;
   if (o.precision < HEOM_FP64_EXACT || o.precision > HEOM_FP32_BULK) return fail(HEOM_ERR_ARG, "unknown precision");
+  if (h->p.dynamics && o.precision != HEOM_FP64_EXACT)
+    return fail(HEOM_ERR_UNSUPPORTED, "population-dynamics keys run on HEOM_FP64_EXACT plans");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0)
@@ -373,8 +400,11 @@ int heom_plan_create(const heom_problem *h, const heom_opts *opts, heom_plan **o
   a.h = hs;
   for (int m = 0; m < 4; m++) a.hb[m] = hs * b[m];
   pl->use_smem = heom_dev::exact_smem_bytes(N, p.n_ado) <= 200 * 1024;
-  int rc = heom_dev::scan_init(pl->scan, p, pl->precision, pl->max_points, o.autotune != 0, pl->stream);
-  if (rc) return fail(rc, heom_dev::scan_last_error());
+  int rc = 0;
+  if (!p.dynamics) { // the batched paths put site j's S on level j+1 (2DES keys only)
+    rc = heom_dev::scan_init(pl->scan, p, pl->precision, pl->max_points, o.autotune != 0, pl->stream);
+    if (rc) return fail(rc, heom_dev::scan_last_error());
+  }
   rc = upload_system(pl.get());
   if (rc) return rc;
   char buf[256];
@@ -422,8 +452,44 @@ int heom_run_traj(heom_plan *pl, int nv1, int nv2, int nv3, double *P, int cap, 
   return HEOM_OK;
 }
 
+int heom_run_populations(heom_plan *pl, const int *sites, int n_sites, double *pop, int cap, int *n_out) {
+  if (!pl || !sites || !n_out || n_sites < 1) return fail(HEOM_ERR_ARG, "bad argument");
+  if (n_sites > heom_plan::kMaxTraj) return fail(HEOM_ERR_CAPACITY, "at most 64 sites per call");
+  if (pl->precision != HEOM_FP64_EXACT)
+    return fail(HEOM_ERR_UNSUPPORTED, "heom_run_populations needs a HEOM_FP64_EXACT plan");
+  const heom::Problem &p = pl->prob;
+  const int N = p.N(), nn = N * N;
+  for (int k = 0; k < n_sites; k++) // dynamics.cpp:206-215
+    if (sites[k] < 1 || sites[k] > N) return fail(HEOM_ERR_ARG, "site " + std::to_string(sites[k]) + " is out of range");
+  CK(cudaSetDevice(pl->device));
+  // One trajectory per site, all in one launch, each reading out Tr(rho_0 |l><l|): the
+  // reference's trace arithmetic with a one-hot operator adds only exact zeros to
+  // rho_0[l][l], so the readout is the population itself.
+  std::vector<double> X(2 * (size_t)n_sites * nn, 0.0);
+  for (int k = 0; k < n_sites; k++) {
+    const int l = sites[k] - 1;
+    X[2 * ((size_t)k * nn + (size_t)l * N + l)] = 1.0;
+  }
+  CK(pl->d_X3pop.ensure((size_t)n_sites * nn));
+  CK(cudaMemcpyAsync(pl->d_X3pop.ptr, X.data(), sizeof(double) * X.size(), cudaMemcpyHostToDevice, pl->stream));
+  std::vector<const double2 *> X3s(n_sites);
+  for (int k = 0; k < n_sites; k++) X3s[k] = pl->d_X3pop.ptr + (size_t)k * nn;
+  std::vector<int> masks(3 * (size_t)n_sites, 0);
+  const double tau[3] = {p.pulses[0].tau0, p.pulses[1].tau0, -HUGE_VAL}; // record from t_start
+  std::vector<std::vector<double>> out;
+  int rc = run_exact(pl, reinterpret_cast<const int(*)[3]>(masks.data()), n_sites, out, tau, X3s.data());
+  if (rc) return rc;
+  const int n = (int)(out[0].size() / 2);
+  *n_out = n;
+  if (n > cap || (!pop && n > 0)) return fail(HEOM_ERR_CAPACITY, "output buffer too small");
+  for (int k = 0; k < n_sites; k++)
+    for (int j = 0; j < n; j++) pop[(size_t)k * cap + j] = out[k][2 * (size_t)j];
+  return HEOM_OK;
+}
+
 int heom_run_2des(heom_plan *pl, double *P, double *p_traj, int cap, int *n_out) {
   if (!pl || !n_out) return fail(HEOM_ERR_ARG, "null argument");
+  if (pl->prob.dynamics) return fail(HEOM_ERR_UNSUPPORTED, "a population-dynamics plan runs heom_run_populations only");
   CK(cudaSetDevice(pl->device));
   static const int masks[3][3] = {{1, 1, 1}, {1, 1, 0}, {1, 0, 1}}; // CPU_2DES.cpp:65-71
   if (pl->precision != HEOM_FP64_EXACT) {
@@ -460,6 +526,7 @@ int heom_run_2des(heom_plan *pl, double *P, double *p_traj, int cap, int *n_out)
 int heom_scan_layout(const heom_plan *pl, const heom_scan_point *pts, int n, long long *offsets, int *counts,
                      long long *total) {
   if (!pl || (!pts && n > 0) || !offsets || !counts || n < 0) return fail(HEOM_ERR_ARG, "bad argument");
+  if (pl->prob.dynamics) return fail(HEOM_ERR_UNSUPPORTED, "a population-dynamics plan runs heom_run_populations only");
   long long off = 0;
   for (int i = 0; i < n; i++) {
     offsets[i] = off;
@@ -473,6 +540,7 @@ int heom_scan_layout(const heom_plan *pl, const heom_scan_point *pts, int n, lon
 int heom_run_scan(heom_plan *pl, const heom_scan_point *pts, int n, double *P, const long long *offsets,
                   const int *counts) {
   if (!pl || (!pts && n > 0) || !P || !offsets || !counts || n < 0) return fail(HEOM_ERR_ARG, "bad argument");
+  if (pl->prob.dynamics) return fail(HEOM_ERR_UNSUPPORTED, "a population-dynamics plan runs heom_run_populations only");
   if (n > pl->max_points) return fail(HEOM_ERR_CAPACITY, "more scan points than the plan's max_points");
   CK(cudaSetDevice(pl->device));
   long long total = 0;
@@ -487,6 +555,7 @@ int heom_run_scan(heom_plan *pl, const heom_scan_point *pts, int n, double *P, c
 
 int heom_run_scan_device(heom_plan *pl, const heom_scan_point *d_pts, int n, double *d_P, const long long *d_offsets) {
   if (!pl || (!d_pts && n > 0) || !d_P || !d_offsets || n < 0) return fail(HEOM_ERR_ARG, "bad argument");
+  if (pl->prob.dynamics) return fail(HEOM_ERR_UNSUPPORTED, "a population-dynamics plan runs heom_run_populations only");
   if (n > pl->max_points) return fail(HEOM_ERR_CAPACITY, "more scan points than the plan's max_points");
   CK(cudaSetDevice(pl->device));
   int rc = heom_dev::scan_run_device(pl->scan, d_pts, n, d_P, d_offsets, pl->stream);
@@ -522,6 +591,7 @@ int heom_adjoint_scan(heom_plan *pl, const heom_scan_point *pts, int n, const lo
                       const double *dLdP, double *P, double *grad) {
   if (!pl || (!pts && n > 0) || !offsets || !dLdP || !P || !grad || n < 0 || total < 0)
     return fail(HEOM_ERR_ARG, "bad argument");
+  if (pl->prob.dynamics) return fail(HEOM_ERR_UNSUPPORTED, "a population-dynamics plan runs heom_run_populations only");
   CK(cudaSetDevice(pl->device));
   int rc = heom_dev::adjoint_scan(pl->prob, pts, n, offsets, total, dLdP, P, grad, &pl->launches, pl->stream);
   if (rc) return fail(rc, heom_dev::adj_last_error());

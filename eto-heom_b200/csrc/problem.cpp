@@ -82,7 +82,109 @@ struct Reader {
 };
 } // namespace
 
+// Population-dynamics key file: param::param_dynamics (param.cpp:250-348).  Every level
+// is a site; the bath's reorganisation energy shifts the first K diagonal elements; the
+// state starts in |1><1| (reset_rho) and evolves under the static H.
+static bool parse_key_dynamics(const std::string &path, Problem &p, std::string &err, int *code) {
+  Reader rd;
+  rd.f.open(path);
+  if (!rd.f) {
+    err = "cannot open key file '" + path + "'";
+    *code = HEOM_ERR_IO;
+    return false;
+  }
+  p = Problem();
+  p.dynamics = true;
+  p.level0 = 0;
+  p.single_manifold = true;
+  bool saw_size = false, saw_ham = false, saw_time = false;
+  std::string kw;
+  auto fail = [&](const std::string &m) { err = m; *code = HEOM_ERR_PARSE; return false; };
+  while (rd.next()) {
+    const std::string &line = rd.line;
+    if (line.empty() || line[0] == '#') continue;
+    { std::istringstream iss(line); iss >> kw; }
+    if (kw == "HEOM") {
+      rd.next();
+      std::istringstream v(rd.line);
+      v >> p.K >> p.L;
+    } else if (kw == "SIZE") {
+      rd.next();
+      std::istringstream v(rd.line);
+      v >> p.single_size;
+      if (p.single_size < 1 || p.single_size > 64) return fail("SIZE must be between 1 and 64");
+      p.sys_size = p.single_size;
+      p.d_a.assign(p.sys_size, 0);
+      p.d_b.assign(p.sys_size, 0);
+      saw_size = true;
+    } else if (kw == "HAMILTONIAN") {
+      if (!saw_size) return fail("HAMILTONIAN before SIZE");
+      const int N = p.sys_size;
+      p.Hkey.assign(2 * (size_t)N * N, 0.0);
+      for (int i = 0; i < p.single_size; i++) {
+        rd.next();
+        std::istringstream row(rd.line);
+        double x;
+        for (int j = 0; row >> x; j++)
+          if (j < N) re(p.Hkey, N, i, j) = x / kHbar;
+      }
+      saw_ham = true;
+    } else if (kw == "TEMPERATURE") {
+      rd.next(); // beta is not used by the propagation
+    } else if (kw == "BATH") {
+      if (!saw_ham) return fail("BATH before HAMILTONIAN (the reorganisation shift needs H)");
+      rd.next();
+      double l = 0;
+      { std::istringstream v(rd.line); v >> l; }
+      const int N = p.sys_size;
+      if (p.K < 1 || p.K > N) return fail("HEOM K must be between 1 and SIZE");
+      for (int i = 0; i < p.K; i++) { // param.cpp:309: H_ii <- Re H_ii + lambda
+        re(p.Hkey, N, i, i) = re(p.Hkey, N, i, i) + l;
+        im(p.Hkey, N, i, i) = 0.0;
+      }
+      rd.next();
+      int nm = 0;
+      { std::istringstream v(rd.line); v >> nm; }
+      if (nm < 1 || nm > 64) return fail("BATH line count must be between 1 and 64");
+      p.alpha.assign(2 * nm, 0.0);
+      p.alpha_t.assign(2 * nm, 0.0);
+      p.gamma.assign(2 * nm, 0.0);
+      for (int k = 0; k < nm; k++) {
+        rd.next();
+        std::istringstream v(rd.line);
+        double a = 0, b = 0, g = 0, w = 0;
+        v >> a >> b >> g >> w;
+        p.alpha[2 * k] = a; p.alpha[2 * k + 1] = b;
+        p.alpha_t[2 * k] = a; p.alpha_t[2 * k + 1] = -b;
+        p.gamma[2 * k] = g; p.gamma[2 * k + 1] = w;
+      }
+      p.K_m = nm;
+      p.have_bath = true;
+    } else if (kw == "TIME") {
+      rd.next();
+      std::istringstream v(rd.line);
+      v >> p.t_start >> p.t_end >> p.step_size >> p.print_step;
+      saw_time = true;
+    }
+  }
+  if (!saw_size || !saw_ham) return fail("key file lacks SIZE or HAMILTONIAN");
+  if (!p.have_bath) return fail("key file lacks a BATH block");
+  if (!saw_time || !(p.step_size > 0) || p.print_stride() <= 0 || !(p.t_end >= p.t_start))
+    return fail("TIME needs t_end >= t_start, step_size > 0 and print_step >= step_size");
+  if (p.L < 0 || p.L > 32) return fail("HEOM depth L must be between 0 and 32");
+  if (p.K * p.K_m > 255) return fail("K * K_m above 255");
+  p.n_sample = 1;
+  p.bath_scale.assign((size_t)p.K * p.K_m, 1.0);
+  build_hierarchy(p);
+  if (p.n_ado <= 0) return fail("empty hierarchy");
+  p.H = p.Hkey;
+  for (auto &X : p.X) X.assign(2 * (size_t)p.N() * p.N(), 0.0);
+  for (Pulse &q : p.pulses) q.taup = 1.0;
+  return true;
+}
+
 bool parse_key(const std::string &path, int flags, Problem &p, std::string &err, int *code) {
+  if (flags & HEOM_KEY_DYNAMICS) return parse_key_dynamics(path, p, err, code);
   Reader rd;
   rd.f.open(path);
   if (!rd.f) {
@@ -367,8 +469,8 @@ void build_hierarchy(Problem &p) {
         const double a1r = x * 0.0, a1i = x * -1.0;
         // S_j rho+: alpha = (x*0, x*1); zgemm first forms temp = alpha * S[s][s].
         const double a2r = x * 0.0, a2i = x * 1.0;
-        p.ops.push_back(CouplingOp{CouplingOp::kCol, j + 1, t, 0, a1r, a1i});
-        p.ops.push_back(CouplingOp{CouplingOp::kRow, j + 1, t, 0, a2r * 1.0 - a2i * 0.0, a2r * 0.0 + a2i * 1.0});
+        p.ops.push_back(CouplingOp{CouplingOp::kCol, j + p.level0, t, 0, a1r, a1i});
+        p.ops.push_back(CouplingOp{CouplingOp::kRow, j + p.level0, t, 0, a2r * 1.0 - a2i * 0.0, a2r * 0.0 + a2i * 1.0});
       }
     if (n != 0)
       for (int j = 0; j < K; j++)
@@ -385,8 +487,8 @@ void build_hierarchy(Problem &p) {
           double x1r = 0.0 * ur - 1.0 * ui, x1i = 0.0 * ui + 1.0 * ur;   // ICNT * (.)
           double vr = y * (sc * p.alpha_t[2 * k]), vi = y * (sc * p.alpha_t[2 * k + 1]);
           double x2r = 0.0 * vr - (-1.0) * vi, x2i = 0.0 * vi + (-1.0) * vr; // MINUS_ICNT * (.)
-          CouplingOp c1{CouplingOp::kRow, j + 1, t, 0, x1r * 1.0 - x1i * 0.0, x1r * 0.0 + x1i * 1.0};
-          CouplingOp c2{CouplingOp::kCol, j + 1, t, 0, x2r, x2i};
+          CouplingOp c1{CouplingOp::kRow, j + p.level0, t, 0, x1r * 1.0 - x1i * 0.0, x1r * 0.0 + x1i * 1.0};
+          CouplingOp c2{CouplingOp::kCol, j + p.level0, t, 0, x2r, x2i};
           p.ops.push_back(c1);
           p.ops.push_back(c2);
         }
@@ -410,6 +512,7 @@ int steps_for(const Problem &p, float t_end) {
 
 // ------------------------------------------------------------------ sample
 void prepare_sample(Problem &p, bool draw, bool rotate) {
+  if (p.dynamics) return; // static H, no orientation: CPU_dynamics draws nothing
   const int N = p.N(), s = p.single_size;
   // construct_Hal (dynamics.cpp:3-51)
   cbuf dH(2 * (size_t)N * N, 0.0);

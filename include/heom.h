@@ -56,7 +56,13 @@ enum { HEOM_MAT_H = 0, HEOM_MAT_X0 = 1, HEOM_MAT_X1 = 2, HEOM_MAT_X2 = 3, HEOM_M
        HEOM_MAT_HKEY = 5 };
 
 /* heom_problem_from_key flags. */
-enum { HEOM_KEY_SINGLE_MANIFOLD = 1 }; /* no two-exciton block (also: MANIFOLD single) */
+enum {
+  HEOM_KEY_SINGLE_MANIFOLD = 1, /* no two-exciton block (also: MANIFOLD single) */
+  HEOM_KEY_DYNAMICS = 2         /* a population-dynamics key (param::param_dynamics,
+                                   param.cpp:250-348): SIZE levels, all of them sites,
+                                   static H with the reorganisation shift, no disorder,
+                                   dipoles or pulses; run with heom_run_populations */
+};
 
 typedef struct heom_problem heom_problem;
 typedef struct heom_plan heom_plan;
@@ -82,6 +88,12 @@ int heom_problem_info_get(const heom_problem *p, heom_problem_info *info);
  * CPU_2DES.cpp:52-60 does: construct_Hal (dynamics.cpp:3-51), polar_mat_set,
  * polar_mat_ranrot, compute_pulse_interaction (polar.cpp:17-101). */
 int heom_problem_prepare_sample(heom_problem *p);
+/* 1 if the two problems' key files differ at most in the pulse central times and the end
+ * time (the fields script/IO-scripts/gen_2d_data.sh:21-33 substitutes into
+ * key.key-tmpl), 0 otherwise: such keys draw the same disorder/orientation samples
+ * (same seed, CPU_2DES.cpp:23-29) and can run as one heom_run_scan batch.  No
+ * counterpart in the reference, which runs one process per key. */
+int heom_problem_scan_compatible(const heom_problem *a, const heom_problem *b);
 /* Same without random draws: zero disorder and no orientational rotation. */
 int heom_problem_prepare_identity(heom_problem *p);
 int heom_problem_reset_rng(heom_problem *p);
@@ -109,6 +121,14 @@ int heom_plan_update(heom_plan *plan, const heom_problem *p);
  * dynamics.cpp:298-432; HEOM_dynamics.cu:489-658).  P receives the recorded
  * Tr(rho_0 X[3]) points, *n_out their count. */
 int heom_run_traj(heom_plan *plan, int nv1, int nv2, int nv3, double *P, int cap, int *n_out);
+
+/* Population dynamics (replaces dynamics_solver, dynamics.cpp:202-295, and the
+ * CPU_dynamics main, etoheom-cpu/src/CPU_dynamics.cpp:14-50): propagates rho from
+ * |1><1| (site 1 excited) under the static H with no fields and records Re rho_0[s][s]
+ * for each site s (1-based) every print_step from t_start.  HEOM_FP64_EXACT plans only
+ * (bit-identical to the reference build); pop receives [n_sites][cap] values and *n_out
+ * the number recorded per site.  Any key works; for a 2DES key the state stays |0><0|. */
+int heom_run_populations(heom_plan *plan, const int *sites, int n_sites, double *pop, int cap, int *n_out);
 
 /* One 2DES point of the current sample: trajectories 111, 110, 101 and
  * P = p111 - p110 - p101 (CPU_2DES.cpp:65-79).  p_traj (optional) receives the

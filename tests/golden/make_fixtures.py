@@ -76,6 +76,17 @@ def key_text(size, K, L, H, bath, dipoles, pulses, time, n_sample=1, seed=7, sig
     return "\n".join(out) + "\n"
 
 
+def dynamics_key_text(H, K, L, bath, time):
+    """A population-dynamics key file (the format of param::param_dynamics,
+    etoheom-cpu/lib/param.cpp:250-348: no ground state, no disorder, dipoles or pulses)."""
+    out = ["# synthetic population-dynamics fixture (tests/golden/make_fixtures.py)", "SIZE", str(len(H)), "",
+           "HEOM", f"{K} {L}", "", "HAMILTONIAN"]
+    out += [" ".join(f"{v:.10g}" for v in row) for row in H]
+    out += ["", "BATHTYPE", "ohmic", "", "TEMPERATURE", "77", "", "BATH", bath[0], str(len(bath[1]))] + list(bath[1])
+    out += ["", "TIME ", " ".join(f"{v:g}" for v in time)]
+    return "\n".join(out) + "\n"
+
+
 def dimer_H():
     return [[0, 0, 0], [0, 12400, 100], [0, 100, 12600]]
 
@@ -171,6 +182,18 @@ def write_keys():
                                           [(210, 20, 500), (260, 20, 500), (260, 20, 500)], (0, 900, 2, 10),
                                           n_sample=2, seed=114,
                                           sigma=[[0, 0, 0], [0, 42.4, 0], [0, 0, 42.4]])
+    # Delay-scan template with disorder averaging (2 samples) for the heom_scan driver
+    # (TAU1..3 / T_END substituted as script/IO-scripts/gen_2d_data.sh does).
+    files["t_scan.key-tmpl"] = (dimer_key(tau=(30, 60, 90), t_end=140, n_sample=2, seed=114,
+                                          sigma=[[0, 0, 0], [0, 42.4, 0], [0, 0, 42.4]])
+                                .replace("30 20 12500", "TAU1 20 12500", 1)
+                                .replace("60 20 12500", "TAU2 20 12500", 1)
+                                .replace("90 20 12500", "TAU3 20 12500", 1)
+                                .replace("0 140 0.5 0.5", "0 T_END 0.5 0.5"))
+    # Population dynamics (CPU_dynamics): a dimer and a trimer, site 1 initially excited.
+    files["d_dimer.key"] = dynamics_key_text([[0, 80], [80, 150]], 2, 3, OHMIC_35_106_77K, (0, 400, 1, 5))
+    files["d_trimer.key"] = dynamics_key_text([[150, 95, -30], [95, 0, 60], [-30, 60, 300]], 3, 3,
+                                              REF_EXAMPLE_BATH, (0, 200, 0.5, 2))
     # Large first-order field (no perturbative smallness) and a negative site energy,
     # which the reference's diagonal sort treats specially (dynamics.cpp:24-27).
     files["t_strong.key"] = key_text(3, 2, 3, [[0, 0, 0], [0, -50, 300], [0, 300, 400]], OHMIC_35_106_77K,
@@ -204,8 +227,29 @@ def parse_driver_output(text):
     return traj, np.array(comb, dtype=np.complex128)
 
 
+DYNAMICS = ["d_dimer.key", "d_trimer.key"]
 GOLDEN = ["c0_dimer_short.key", "c0_dimer.key", "c4_trimer_short.key", "t_disorder.key",
           "t_ref_example.key", "t_strong.key", "c1_fmo_short.key"]
+
+
+# The delay scan of the heom_scan driver test (gen_2d_data.sh parameters).
+SCAN_ARGS = dict(t0=30, propagate=40, tau_step=10, tau_bound=20, T=("0", "50"))
+
+
+def gen_2d_keys(template_text, t0, propagate, tau_step, tau_bound, T):
+    """Restatement of script/IO-scripts/gen_2d_data.sh:37-61: {file name: key text}."""
+    def emit(tau1, tau2, tau3, t_end):
+        return (template_text.replace("TAU1", str(tau1)).replace("TAU2", str(tau2))
+                .replace("TAU3", str(tau3)).replace("T_END", str(t_end)))
+    out = {}
+    for t in T:
+        tv = int(t)
+        for i in range(0, tau_bound + 1, tau_step):
+            out[f"key_{i}_{t}.key"] = emit(t0, t0 + i, t0 + i + tv, t0 + i + tv + propagate)
+        for i in range(-tau_bound, 0, tau_step):
+            a = -i
+            out[f"key_{i}_{t}.key"] = emit(t0 + a, t0, t0 + a + tv, t0 + a + tv + propagate)
+    return out
 
 
 def write_golden():
@@ -224,6 +268,33 @@ def write_golden():
         out = subprocess.run([exe, os.path.join(KEYS, name)], check=True, capture_output=True, text=True).stdout
         with open(os.path.join(REF, name.replace(".key", ".out")), "w") as f:
             f.write(out)
+    # Population dynamics: full-precision populations (ref_dynamics) and CPU_dynamics stdout.
+    dyn = os.path.join(ROOT, "oracle", "_ref", "ref_dynamics")
+    cdyn = os.path.join(ROOT, "oracle", "_ref", "CPU_dynamics")
+    for name in DYNAMICS:
+        kp = os.path.join(KEYS, name)
+        out = subprocess.run([dyn, kp, "1", "2"], check=True, capture_output=True, text=True).stdout
+        pops = [[float(x) for x in blk.split("\n")[1:] if x.strip()] for blk in out.split("#site")[1:]]
+        np.savez_compressed(os.path.join(REF, name.replace(".key", ".npz")), population=np.array(pops))
+        # CPU_dynamics prints "Running <path>": run it from the key's directory with the bare name
+        txt = subprocess.run([cdyn, name], cwd=KEYS, check=True, capture_output=True, text=True).stdout
+        with open(os.path.join(REF, name.replace(".key", ".out")), "w") as f:
+            f.write(txt)
+        print(f"{name}: populations {np.array(pops).shape}")
+    # CPU_2DES outputs of the driver's delay scan: 2d-output/out_{tau}_{T}.out
+    import tempfile
+    scan_out = os.path.join(REF, "scan")
+    os.makedirs(scan_out, exist_ok=True)
+    keys = gen_2d_keys(open(os.path.join(KEYS, "t_scan.key-tmpl")).read(), **SCAN_ARGS)
+    with tempfile.TemporaryDirectory() as d:
+        for name, text in sorted(keys.items()):
+            kp = os.path.join(d, name)
+            with open(kp, "w") as f:
+                f.write(text)
+            out = subprocess.run([exe, kp], check=True, capture_output=True, text=True).stdout
+            with open(os.path.join(scan_out, "out" + name[3:-4] + ".out"), "w") as f:
+                f.write(out)
+    print(f"scan: {len(keys)} CPU_2DES outputs")
 
 
 if __name__ == "__main__":
