@@ -41,9 +41,9 @@ METRIC = "2DES propagations/sec, chosen vs plain FP64 on 1 B200 at ≤1e-6 P(t) 
 UNIT = "propagations/s"
 KEY = os.path.join(ROOT, "tests", "golden", "keys", "c0_dimer.key")
 # dram__bytes_read.sum + dram__bytes_write.sum of the scan kernel from one ncu capture of
-# `bench.py --profile-run fp32-bulk` (418,304 B over 92,768 point-steps), scaled to a full
+# `bench.py --profile-run fp32-bulk` (105,216 B over 92,768 point-steps), scaled to a full
 # launch by point-steps (inputs, tables and P(t) scale with points and steps).
-DRAM_BYTES_PER_POINT_STEP = 418304.0 / 92768.0
+DRAM_BYTES_PER_POINT_STEP = 105216.0 / 92768.0
 TEMPLATE = os.path.join(ROOT, "tests", "golden", "keys", "c2_dimer_scan.key-tmpl")
 
 

@@ -59,6 +59,7 @@ template <int NT> __host__ __device__ inline size_t pm_smem_bytes(size_t tsz, in
   b += al16((tsz == 4 ? 16 : 32) * nM); // links ([o][n])
   b += al16(16 * (size_t)NN);           // off-diagonal H (FP64)
   b += al16(16 * 3 * (size_t)NN);       // X0, X1^T, X2^T (FP64)
+  b += al16(16 * (size_t)n_ado);        // damping scalars
   b += al16(16 * 3 * (size_t)wcap);     // pulse-field windows
   return b;
 }
@@ -256,12 +257,12 @@ __device__ __forceinline__ void pm_stage(const PmShared &g, int cc, int n, int t
 template <typename T, int NT, int RPT, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1) scan_pm(ScanArgs a) {
   using T2 = typename V2<T>::t;
-  constexpr int NN = NT * NT, GPR = NT / RPT;
-  static_assert(NT % RPT == 0 && GPR <= 4, "rows per thread must divide N");
+  constexpr int NN = NT * NT;
+  static_assert(RPT == NT, "one thread per whole block");
   static_assert(NN <= 32, "warp 0 builds A with one lane per element");
   static_assert(NT <= 4, "levels 1..3 carry the bath couplings");
   extern __shared__ __align__(16) unsigned char sm[];
-  __shared__ double2 s_tr[8];
+  __shared__ double2 s_tr[2];
   __shared__ unsigned s_mask[6];
   __shared__ int s_lo[3], s_cnt[3], s_point, s_rstat;
   const int M = a.M, nado = a.n_ado, K = a.K, Km = a.K_m, wcap = a.wcap, ado0 = a.ado0;
@@ -286,6 +287,8 @@ __global__ void __launch_bounds__(MAXT, 1) scan_pm(ScanArgs a) {
   p += al16(16 * (size_t)NN);
   double2 *Xf = (double2 *)p; // X0, X1^T, X2^T
   p += al16(16 * 3 * (size_t)NN);
+  double2 *sdamp = (double2 *)p; // damping scalar per ADO
+  p += al16(16 * (size_t)nado);
   double2 *fwin = (double2 *)p; // [3][wcap]
   TableLayout tl(nado, M, Km);
   const PmLinkHost *g_link = (const PmLinkHost *)(a.tables + tl.plink);
@@ -299,6 +302,7 @@ __global__ void __launch_bounds__(MAXT, 1) scan_pm(ScanArgs a) {
     v.ud = L.ud;
     links[q] = v;
   }
+  for (int q = tid; q < nado; q += bs) sdamp[q] = g_damp[q];
   const double *g_Hd = a.sys, *g_Hoff = a.sys + NT, *g_Xs = g_Hoff + 2 * NN, *g_X3 = g_Xs + 6 * NN;
   for (int q = tid; q < NN; q += bs) {
     X3[q] = make_double2(g_X3[2 * q], g_X3[2 * q + 1]);
@@ -313,11 +317,6 @@ __global__ void __launch_bounds__(MAXT, 1) scan_pm(ScanArgs a) {
            g_Hoff[2 * j * NT + 1] == 0.0;
     s_rstat = z;
   }
-  const bool active = tid < S * GPR;
-  const int blkid = active ? tid % S : 0;      // block = cc * nado + n
-  const int grp = active ? tid / S : 0;        // row group
-  const int cc = blkid / nado, n = blkid - cc * nado;
-  const double2 dmp = active ? g_damp[n] : make_double2(0.0, 0.0);
   const PmShared gsh{SP, nado, M, K, Km};
 
   for (;;) {
@@ -355,18 +354,14 @@ __global__ void __launch_bounds__(MAXT, 1) scan_pm(ScanArgs a) {
       s_lo[q] = lo < 0 ? 0 : lo;
       s_cnt[q] = cnt;
     }
-    // initial state: R = |0><0| on ADO 0, D2 = D3 = Q = 0
-    double2 w64[RPT * NT];
-#pragma unroll
-    for (int e = 0; e < RPT * NT; e++) {
-      const int q = grp * RPT * NT + e;
-      const double v = (blkid == ado0 && q == 0 && active) ? 1.0 : 0.0;
-      w64[e] = make_double2(v, 0.0);
-      if (active) { // both copies: a dormant component never rewrites either
-        rho[q * SP + blkid] = w64[e];
-        w32[q * SP + blkid] = mk2<T>(v, 0.0);
-        w32[EP + q * SP + blkid] = mk2<T>(v, 0.0);
-      }
+    // initial state: R = |0><0| on ADO 0, D2 = D3 = Q = 0 (both FP32 copies: a dormant
+    // component never rewrites either)
+    for (size_t e = tid; e < (size_t)NN * S; e += bs) {
+      const size_t q = e / S, blk = e - q * S;
+      const double v = (blk == (size_t)ado0 && q == 0) ? 1.0 : 0.0;
+      rho[q * SP + blk] = make_double2(v, 0.0);
+      w32[q * SP + blk] = mk2<T>(v, 0.0);
+      w32[EP + q * SP + blk] = mk2<T>(v, 0.0);
     }
     __syncthreads();
     for (int q = 0; q < 3; q++) {
@@ -375,24 +370,26 @@ __global__ void __launch_bounds__(MAXT, 1) scan_pm(ScanArgs a) {
     }
     const int lo1 = s_lo[0], lo2 = s_lo[1], lo3 = s_lo[2];
     const int cn1 = s_cnt[0], cn2 = s_cnt[1], cn3 = s_cnt[2];
-    // First step at which this thread's component can leave its initial value.
+    // First step at which each component can leave its initial value.
     constexpr int kNever = 0x7fffffff;
     const int wR = s_rstat ? (cn1 > 0 ? lo1 : kNever) : 0;
     const int wD2 = cn2 > 0 ? lo2 : kNever, wD3 = cn3 > 0 ? lo3 : kNever;
     int wQ = kNever;
     if (cn2 > 0 && wD3 != kNever && max(lo2, wD3) < lo2 + cn2) wQ = max(lo2, wD3);
     if (cn3 > 0 && wD2 != kNever && max(lo3, wD2) < lo3 + cn3) wQ = min(wQ, max(lo3, wD2));
-    const int wake = cc == 0 ? wR : cc == 1 ? wD2 : cc == 2 ? wD3 : wQ;
     int buf = 0, rec = 0;
     float t = a.t_start;
     for (int i = 0; i < nsteps; i++) {
       const int on1 = (unsigned)(i - lo1) < (unsigned)cn1, on2 = (unsigned)(i - lo2) < (unsigned)cn2,
                 on3 = (unsigned)(i - lo3) < (unsigned)cn3;
+      const bool do_rec = t >= pt.tau3 && i % a.stride == 0;
       if (i == 0) __syncthreads(); // field tables complete
       if (tid < 32) {
-        // warp 0: A of the four components, the two pulse operators and their masks
+        // warp 0: A of the four components, the two pulse operators and their masks;
+        // P = Tr(X3 (Q - R)) on ADO 0 before the step, one element per lane (FP64)
         const int q = tid;
         bool nz[6] = {false, false, false, false, false, false};
+        double2 cR = make_double2(0.0, 0.0), cQ = make_double2(0.0, 0.0);
         if (q < NN) {
           const int ons[3] = {on1, on2, on3}, los[3] = {lo1, lo2, lo3}, cns[3] = {cn1, cn2, cn3};
           double vr[3], vi[3];
@@ -417,62 +414,66 @@ __global__ void __launch_bounds__(MAXT, 1) scan_pm(ScanArgs a) {
             Aall[s * NN + q] = v[s];
             nz[s] = v[s].x != (T)0 || v[s].y != (T)0;
           }
+          if (do_rec) { // element (j, l) contributes rho[j][l] X3[l][j]
+            const int j = q / NT, l = q - j * NT;
+            const double2 x = X3[l * NT + j], r = rho[q * SP + ado0], z = rho[q * SP + 3 * nado + ado0];
+            cR = make_double2(r.x * x.x - r.y * x.y, r.x * x.y + r.y * x.x);
+            cQ = make_double2(z.x * x.x - z.y * x.y, z.x * x.y + z.y * x.x);
+          }
         }
 #pragma unroll
         for (int s = 0; s < 6; s++) {
           const unsigned b = __ballot_sync(0xffffffffu, nz[s]);
           if (q == 0) s_mask[s] = b;
         }
-      }
-      // P = Tr(X3 (Q - R)) on ADO 0 before the step: each owner of a row group of
-      // R_0 or Q_0 traces its rows (FP64); thread 0 combines after the barrier.
-      const bool do_rec = t >= pt.tau3 && i % a.stride == 0;
-      if (do_rec && active && n == ado0 && (cc == 0 || cc == 3)) {
-        double sr = 0.0, si = 0.0;
+        if (do_rec) {
 #pragma unroll
-        for (int rr = 0; rr < RPT; rr++)
-#pragma unroll
-          for (int l = 0; l < NT; l++) {
-            const int jr = grp * RPT + rr;
-            const double2 v = w64[rr * NT + l], x = X3[l * NT + jr];
-            sr += v.x * x.x - v.y * x.y;
-            si += v.x * x.y + v.y * x.x;
+          for (int o = 16; o >= 1; o >>= 1) {
+            cR.x += __shfl_xor_sync(0xffffffffu, cR.x, o);
+            cR.y += __shfl_xor_sync(0xffffffffu, cR.y, o);
+            cQ.x += __shfl_xor_sync(0xffffffffu, cQ.x, o);
+            cQ.y += __shfl_xor_sync(0xffffffffu, cQ.y, o);
           }
-        s_tr[(cc == 0 ? 0 : 4) + grp] = make_double2(sr, si);
+          if (q == 0) {
+            s_tr[0] = cR;
+            s_tr[1] = cQ;
+          }
+        }
       }
       __syncthreads();
       if (do_rec) {
-        if (tid == 0) {
-          double pr = 0.0, pim = 0.0;
-          for (int q = 0; q < GPR; q++) {
-            pr += s_tr[4 + q].x - s_tr[q].x;
-            pim += s_tr[4 + q].y - s_tr[q].y;
-          }
-          a.P[off + rec] = make_double2(pr, pim);
-        }
+        if (tid == 0) a.P[off + rec] = make_double2(s_tr[1].x - s_tr[0].x, s_tr[1].y - s_tr[0].y);
         rec++;
       }
-      const unsigned am = s_mask[cc], m2 = s_mask[4], m3 = s_mask[5];
+      // One thread per block of every awake component.  The Horner accumulator restarts
+      // from rho each step (w = rho at the first stage), so no state crosses steps in
+      // registers.  (Spreading one or two awake components over all threads, two per
+      // block, measured slower: the duplicated block loads and the larger code cost
+      // more than the shorter per-thread chains save.)
+      const bool a0 = i >= wR, a1 = i >= wD2, a2 = i >= wD3, a3 = i >= wQ;
+      int cc = -1, n = 0;
+      if (tid < S) {
+        const int c = tid / nado;
+        const bool awake = c == 0 ? a0 : c == 1 ? a1 : c == 2 ? a2 : a3;
+        if (awake) {
+          cc = c;
+          n = tid - c * nado;
+        }
+      }
+      const int blk = cc >= 0 ? cc * nado + n : 0;
+      const double2 dmp = cc >= 0 ? sdamp[n] : make_double2(0.0, 0.0);
+      const unsigned am = cc >= 0 ? s_mask[cc] : 0u, m2 = s_mask[4], m3 = s_mask[5];
       const bool src = (on2 || on3) && cc > 0;
+      double2 w64[NN];
+#pragma unroll
+      for (int e = 0; e < NN; e++) w64[e] = cc >= 0 ? rho[e * SP + blk] : make_double2(0.0, 0.0);
       for (int m = 4; m >= 1; m--) {
         const double cm = a.h / m;
         const T2 *W = w32 + (size_t)buf * EP;
         T2 *Wn = w32 + (size_t)(buf ^ 1) * EP;
-        if (active && i >= wake) {
-          // the row group is warp-uniform except where a warp straddles two groups
-          if (grp == 0)
-            pm_stage<T, NT, RPT, 0>(gsh, cc, n, blkid, src, on2, on3, am, m2, m3, W, Wn, Aall, Hdd, rho, links,
-                                        dmp, cm, m == 1, w64);
-          else if (GPR > 1 && grp == 1)
-            pm_stage<T, NT, RPT, (GPR > 1 ? RPT : 0)>(gsh, cc, n, blkid, src, on2, on3, am, m2, m3, W, Wn, Aall,
-                                                            Hdd, rho, links, dmp, cm, m == 1, w64);
-          else if (GPR > 2 && grp == 2)
-            pm_stage<T, NT, RPT, (GPR > 2 ? 2 * RPT : 0)>(gsh, cc, n, blkid, src, on2, on3, am, m2, m3, W, Wn,
-                                                                Aall, Hdd, rho, links, dmp, cm, m == 1, w64);
-          else if (GPR > 3)
-            pm_stage<T, NT, RPT, (GPR > 3 ? 3 * RPT : 0)>(gsh, cc, n, blkid, src, on2, on3, am, m2, m3, W, Wn,
-                                                                Aall, Hdd, rho, links, dmp, cm, m == 1, w64);
-        }
+        if (cc >= 0)
+          pm_stage<T, NT, NT, 0>(gsh, cc, n, blk, src, on2, on3, am, m2, m3, W, Wn, Aall, Hdd, rho, links, dmp, cm,
+                                 m == 1, w64);
         buf ^= 1;
         __syncthreads();
       }
