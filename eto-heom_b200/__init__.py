@@ -56,7 +56,7 @@ class ProblemInfo(ctypes.Structure):
 
 class Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("device", ctypes.c_int), ("stream", ctypes.c_void_p),
-                ("max_points", ctypes.c_int), ("autotune", ctypes.c_int)]
+                ("max_points", ctypes.c_int), ("autotune", ctypes.c_int), ("single_pass", ctypes.c_int)]
 
 
 class ScanPoint(ctypes.Structure):
@@ -217,10 +217,11 @@ class Plan:
     """A device plan for one problem (one CUDA device and stream)."""
 
     def __init__(self, problem: Problem, precision="fp64-exact", device: int = 0, max_points: int = 1024,
-                 autotune: bool = False, stream: int | None = None):
+                 autotune: bool = False, stream: int | None = None, single_pass: bool = False):
         self.problem = problem
         prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
-        o = Opts(prec, device, ctypes.c_void_p(stream) if stream else None, max_points, 1 if autotune else 0)
+        o = Opts(prec, device, ctypes.c_void_p(stream) if stream else None, max_points, 1 if autotune else 0,
+                 1 if single_pass else 0)
         h = ctypes.c_void_p()
         _check(lib().heom_plan_create(problem._h, ctypes.byref(o), ctypes.byref(h)))
         self._h = h

@@ -402,7 +402,8 @@ int heom_plan_create(const heom_problem *h, const heom_opts *opts, heom_plan **o
   pl->use_smem = heom_dev::exact_smem_bytes(N, p.n_ado) <= 200 * 1024;
   int rc = 0;
   if (!p.dynamics) { // the batched paths put site j's S on level j+1 (2DES keys only)
-    rc = heom_dev::scan_init(pl->scan, p, pl->precision, pl->max_points, o.autotune != 0, pl->stream);
+    rc = heom_dev::scan_init(pl->scan, p, pl->precision, pl->max_points, o.autotune != 0, pl->stream,
+                             o.single_pass != 0);
     if (rc) return fail(rc, heom_dev::scan_last_error());
   }
   rc = upload_system(pl.get());
@@ -547,9 +548,10 @@ int heom_run_scan(heom_plan *pl, const heom_scan_point *pts, int n, double *P, c
   for (int i = 0; i < n; i++) total = std::max(total, offsets[i] + counts[i]);
   if (!pl->scan.supported) // hierarchy too large for one CTA: staged path
     return run_sg(pl, 4, nullptr, pts, n, P, offsets, total);
+  const long long before = pl->scan.staged_launches;
   int rc = heom_dev::scan_run_host(pl->scan, pts, n, P, offsets, total, pl->stream);
   if (rc) return fail(rc, heom_dev::scan_last_error());
-  pl->launches += heom_dev::scan_launches_per_run(pl->scan);
+  pl->launches += pl->scan.staged ? pl->scan.staged_launches - before : heom_dev::scan_launches_per_run(pl->scan);
   return HEOM_OK;
 }
 
@@ -558,9 +560,10 @@ int heom_run_scan_device(heom_plan *pl, const heom_scan_point *d_pts, int n, dou
   if (pl->prob.dynamics) return fail(HEOM_ERR_UNSUPPORTED, "a population-dynamics plan runs heom_run_populations only");
   if (n > pl->max_points) return fail(HEOM_ERR_CAPACITY, "more scan points than the plan's max_points");
   CK(cudaSetDevice(pl->device));
+  const long long before = pl->scan.staged_launches;
   int rc = heom_dev::scan_run_device(pl->scan, d_pts, n, d_P, d_offsets, pl->stream);
   if (rc) return fail(rc, heom_dev::scan_last_error());
-  pl->launches += heom_dev::scan_launches_per_run(pl->scan);
+  pl->launches += pl->scan.staged ? pl->scan.staged_launches - before : heom_dev::scan_launches_per_run(pl->scan);
   return HEOM_OK;
 }
 

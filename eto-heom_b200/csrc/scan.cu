@@ -721,6 +721,7 @@ __global__ void __launch_bounds__(MAXT, 1) scan_rows(ScanArgs a) {
 }
 
 #include "scan_pm.cuh"
+#include "scan_slots.cuh"
 
 // Order points by descending step count (single CTA, bitonic sort in shared memory).
 __global__ void scan_order(const heom_scan_point *pts, int n, float t_start, float dt, int *order, int *counter) {
@@ -893,6 +894,13 @@ int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
   if (!s.supported) return 0;
   std::vector<double> sys;
   scan_system_host(p, sys);
+  { // the kernels' test for a stationary |0><0| (off-diagonal H in row and column 0)
+    const double *Hoff = sys.data() + s.N;
+    bool z = true;
+    for (int j = 1; j < s.N; j++)
+      z = z && Hoff[2 * j] == 0.0 && Hoff[2 * j + 1] == 0.0 && Hoff[2 * j * s.N] == 0.0 && Hoff[2 * j * s.N + 1] == 0.0;
+    s.rstat = z;
+  }
   cudaError_t e = cudaMemcpyAsync(s.d_sys, sys.data(), sizeof(double) * sys.size(), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) { s_err = std::string("scan system upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
@@ -1099,9 +1107,327 @@ bool scan_prepare(ScanState &s, const heom::Problem &p, int precision, int max_p
   return true;
 }
 
-int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_points, bool tune, cudaStream_t st) {
+// ------------------------------------------------------------------ staged scan
+namespace {
+
+using SlotFn = void (*)(SlotArgs);
+constexpr int kSlotThreads = 320;
+SlotFn slot_kernel(int precision) {
+  return precision == HEOM_FP64 ? scan_slots<double, 4, kSlotThreads> : scan_slots<float, 4, kSlotThreads>;
+}
+constexpr int kNever = 0x7fffffff;
+
+// Per-point schedule, with the kernels' float time grid and window tests.
+struct PtPlan {
+  int nsteps = 0, lo[3] = {0, 0, 0}, cnt[3] = {0, 0, 0};
+  int wR = 0, wD2 = kNever, wD3 = kNever, wQ = kNever;
+  int s2 = kNever, s3 = 0, rs = 0;
+  bool regular = false;
+};
+
+PtPlan plan_point(const ScanState &s, const heom_scan_point &pt) {
+  PtPlan q;
+  const float nstep = (pt.t_end - s.t_start) / s.dt;
+  q.nsteps = nstep >= 0.0f ? (int)nstep + 1 : 0;
+  const double tau[3] = {pt.tau1, pt.tau2, pt.tau3};
+  for (int k = 0; k < 3; k++) {
+    int lo = -1, cnt = 0;
+    float t = s.t_start;
+    for (int i = 0; i < q.nsteps; i++) {
+      const double d = (double)t - tau[k];
+      if (std::fabs(d) <= s.taup[k] * 2) {
+        if (lo < 0) lo = i;
+        cnt++;
+      } else if (lo >= 0) {
+        break;
+      }
+      t += s.dt;
+    }
+    q.lo[k] = lo < 0 ? 0 : lo;
+    q.cnt[k] = cnt;
+  }
+  q.wR = s.rstat ? (q.cnt[0] > 0 ? q.lo[0] : kNever) : 0;
+  q.wD2 = q.cnt[1] > 0 ? q.lo[1] : kNever;
+  q.wD3 = q.cnt[2] > 0 ? q.lo[2] : kNever;
+  if (q.cnt[1] > 0 && q.wD3 != kNever && std::max(q.lo[1], q.wD3) < q.lo[1] + q.cnt[1]) q.wQ = std::max(q.lo[1], q.wD3);
+  if (q.cnt[2] > 0 && q.wD2 != kNever && std::max(q.lo[2], q.wD2) < q.lo[2] + q.cnt[2])
+    q.wQ = std::min(q.wQ, std::max(q.lo[2], q.wD2));
+  q.s2 = std::min(q.wD3, q.wQ);
+  for (int k = 0; k < 3; k++)
+    if (q.cnt[k] > 0) q.s3 = std::max(q.s3, q.lo[k] + q.cnt[k]);
+  q.rs = q.nsteps;
+  float t = s.t_start;
+  for (int i = 0; i < q.nsteps; i++) {
+    if (t >= pt.tau3 && i % s.stride == 0) { q.rs = i; break; }
+    t += s.dt;
+  }
+  // Stageable: D3 and Q wake inside the point, no P record before they do, and every
+  // pulse window closes inside the point.
+  q.regular = q.s2 < q.nsteps && q.s2 <= q.s3 && q.s3 <= q.nsteps && q.rs >= q.s2;
+  return q;
+}
+
+int records_before(const ScanState &s, const heom_scan_point &pt, int upto) {
+  int c = 0;
+  float t = s.t_start;
+  for (int i = 0; i < upto; i++) {
+    if (t >= pt.tau3 && i % s.stride == 0) c++;
+    t += s.dt;
+  }
+  return c;
+}
+
+SlotSpec slot_off() {
+  SlotSpec z{};
+  z.src[0] = z.src[1] = -1;
+  z.wake = z.stop = 0;
+  return z;
+}
+SlotSpec slot_mk(int op, int fset, int wake, int stop, int init, const double2 *init_ptr) {
+  SlotSpec z = slot_off();
+  z.op = op;
+  z.fset = fset;
+  z.wake = wake;
+  z.stop = stop;
+  z.init = init;
+  z.init_ptr = init_ptr;
+  return z;
+}
+SlotRec rec_off() {
+  SlotRec r{};
+  r.q = r.r = -1;
+  return r;
+}
+void set_taus(SlotJob &J, int f, const heom_scan_point &pt) {
+  J.tau[f][0] = pt.tau1;
+  J.tau[f][1] = pt.tau2;
+  J.tau[f][2] = pt.tau3;
+}
+
+} // namespace
+
+// Launch shape of the slot kernel; leaves s.staged false when it does not fit.
+void staged_prepare(ScanState &s) {
+  s.staged = false;
+  if (s.N != 4) return;
+  int dev = 0, max_smem = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const size_t tsz = s.precision == HEOM_FP64 ? 8 : 4;
+  s.sl_wcap = pm_window_cap(s.taup, s.dt);
+  if (sl_smem_bytes<4>(tsz, s.n_ado, s.M, s.sl_wcap) + 1024 > (size_t)max_smem) s.sl_wcap = 0;
+  s.sl_smem = sl_smem_bytes<4>(tsz, s.n_ado, s.M, s.sl_wcap);
+  s.sl_threads = (4 * s.n_ado + 31) / 32 * 32;
+  if (s.sl_smem + 1024 > (size_t)max_smem || s.sl_threads > kSlotThreads || s.n_ado >= 0xffff) return;
+  SlotFn f = slot_kernel(s.precision);
+  if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.sl_smem) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, s.sl_threads, s.sl_smem);
+  s.sl_grid = s.sm_count * std::max(per_sm, 1);
+  s.staged = per_sm > 0;
+}
+
+template <class T> static cudaError_t grow(void *&ptr, size_t &cap, size_t want) {
+  if (want <= cap && ptr) return cudaSuccess;
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  cap = 0;
+  cudaError_t e = cudaMalloc(&ptr, sizeof(T) * std::max<size_t>(want, 1));
+  if (e == cudaSuccess) cap = want;
+  return e;
+}
+
+int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, const long long *offsets,
+               cudaStream_t st) {
+  const int NN = s.N * s.N;
+  const size_t snap_elems = (size_t)NN * s.n_ado; // double2 per state
+  std::vector<PtPlan> pl(n);
+  std::vector<int> regular;
+  for (int i = 0; i < n; i++) {
+    pl[i] = plan_point(s, pts[i]);
+    if (pl[i].regular) regular.push_back(i);
+  }
+  std::vector<long long> snap_of(n, -1); // first of the point's two snapshot states
+  for (size_t k = 0; k < regular.size(); k++) snap_of[regular[k]] = 2 * (long long)k;
+  cudaError_t e = grow<double2>(s.d_snap, s.snap_cap, std::max<size_t>(2 * regular.size(), 1) * snap_elems);
+  if (e != cudaSuccess) { s_err = "staged scan snapshots: out of device memory"; return HEOM_ERR_NOMEM; }
+  double2 *snap = (double2 *)s.d_snap;
+  auto state = [&](int i, int which) { return snap + (size_t)(snap_of[i] + which) * snap_elems; };
+  double2 *P = (double2 *)d_P;
+
+  std::vector<SlotJob> jobs[3];
+  std::vector<SlotSave> saves[3];
+  // stage 1: R and D2 per (tau1, tau2) group up to the members' pulse-3 windows
+  std::vector<int> order(regular);
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    if (pts[a].tau1 != pts[b].tau1) return pts[a].tau1 < pts[b].tau1;
+    if (pts[a].tau2 != pts[b].tau2) return pts[a].tau2 < pts[b].tau2;
+    return pl[a].s2 < pl[b].s2;
+  });
+  for (size_t g0 = 0; g0 < order.size();) {
+    size_t g1 = g0;
+    while (g1 < order.size() && pts[order[g1]].tau1 == pts[order[g0]].tau1 &&
+           pts[order[g1]].tau2 == pts[order[g0]].tau2)
+      g1++;
+    const int lead = order[g0];
+    int last = 0;
+    for (size_t k = g0; k < g1; k++) last = std::max(last, pl[order[k]].s2);
+    const int first = std::min(std::min(pl[lead].wR, pl[lead].wD2), last);
+    SlotJob J{};
+    J.first = first;
+    J.last = last;
+    set_taus(J, 0, pts[lead]);
+    set_taus(J, 1, pts[lead]);
+    J.slot[0] = slot_mk(1, 0, pl[lead].wR, last, 1, nullptr);
+    J.slot[1] = slot_mk(3, 0, pl[lead].wD2, last, 0, nullptr);
+    J.slot[1].src[0] = 0;
+    J.slot[1].srcq[0] = 1;
+    J.slot[2] = J.slot[3] = slot_off();
+    J.rec[0] = J.rec[1] = rec_off();
+    J.save_begin = (int)saves[0].size();
+    for (size_t k = g0; k < g1; k++) { // sorted by s2
+      const int i = order[k];
+      saves[0].push_back(SlotSave{std::max(pl[i].s2, first), 0, state(i, 0)});
+      saves[0].push_back(SlotSave{std::max(pl[i].s2, first), 1, state(i, 1)});
+    }
+    J.save_end = (int)saves[0].size();
+    jobs[0].push_back(J);
+    g0 = g1;
+  }
+  // stage 2: each point's pulse-3 window (regular points) or the whole point (others)
+  for (int i = 0; i < n; i++) {
+    const PtPlan &q = pl[i];
+    const bool reg = q.regular;
+    SlotJob J{};
+    J.first = reg ? q.s2 : 0;
+    J.last = reg ? q.s3 : q.nsteps;
+    if (J.last <= J.first && !reg) continue; // an empty point records nothing
+    set_taus(J, 0, pts[i]);
+    set_taus(J, 1, pts[i]);
+    J.slot[0] = slot_mk(1, 0, std::max(J.first, q.wR), J.last, reg ? 2 : 1, reg ? state(i, 0) : nullptr);
+    J.slot[1] = slot_mk(3, 0, std::max(J.first, q.wD2), J.last, reg ? 2 : 0, reg ? state(i, 1) : nullptr);
+    J.slot[1].src[0] = 0;
+    J.slot[1].srcq[0] = 1;
+    J.slot[2] = slot_mk(5, 0, std::max(J.first, q.wD3), J.last, 0, nullptr);
+    J.slot[2].src[0] = 0;
+    J.slot[2].srcq[0] = 2;
+    J.slot[3] = slot_mk(7, 0, std::max(J.first, q.wQ), J.last, 0, nullptr);
+    J.slot[3].src[0] = 2; // -i[V2, D3], then -i[V3, D2]: the single-pass order
+    J.slot[3].srcq[0] = 1;
+    J.slot[3].src[1] = 1;
+    J.slot[3].srcq[1] = 2;
+    J.rec[0] = rec_off();
+    J.rec[0].q = 3;
+    J.rec[0].r = 0;
+    J.rec[0].first = J.first;
+    J.rec[0].last = J.last;
+    J.rec[0].rec0 = 0;
+    J.rec[0].tau3 = pts[i].tau3;
+    J.rec[0].P = P + offsets[i];
+    J.rec[1] = rec_off();
+    J.save_begin = (int)saves[1].size();
+    if (reg) {
+      saves[1].push_back(SlotSave{J.last, 0, state(i, 0)});
+      saves[1].push_back(SlotSave{J.last, 3, state(i, 1)});
+    }
+    J.save_end = (int)saves[1].size();
+    jobs[1].push_back(J);
+  }
+  // stage 3: pulse-free tails of regular points, two per job, paired by window end
+  std::vector<int> tails;
+  for (int i : regular)
+    if (pl[i].s3 < pl[i].nsteps) tails.push_back(i);
+  std::sort(tails.begin(), tails.end(), [&](int a, int b) {
+    return pl[a].s3 != pl[b].s3 ? pl[a].s3 < pl[b].s3 : pl[a].nsteps < pl[b].nsteps;
+  });
+  for (size_t k = 0; k < tails.size(); k += 2) {
+    SlotJob J{};
+    J.first = kNever;
+    J.last = 0;
+    for (int h = 0; h < 2; h++) {
+      J.slot[2 * h] = J.slot[2 * h + 1] = slot_off();
+      J.rec[h] = rec_off();
+      if (k + h >= tails.size()) { set_taus(J, h, pts[tails[k]]); continue; }
+      const int i = tails[k + h];
+      const PtPlan &q = pl[i];
+      set_taus(J, h, pts[i]);
+      J.first = std::min(J.first, q.s3);
+      J.last = std::max(J.last, q.nsteps);
+      J.slot[2 * h] = slot_mk(1, h, q.s3, q.nsteps, 2, state(i, 0));
+      J.slot[2 * h + 1] = slot_mk(7, h, q.s3, q.nsteps, 2, state(i, 1));
+      J.rec[h].q = 2 * h + 1;
+      J.rec[h].r = 2 * h;
+      J.rec[h].first = q.s3;
+      J.rec[h].last = q.nsteps;
+      J.rec[h].rec0 = records_before(s, pts[i], q.s3);
+      J.rec[h].tau3 = pts[i].tau3;
+      J.rec[h].P = P + offsets[i];
+    }
+    J.save_begin = J.save_end = 0;
+    jobs[2].push_back(J);
+  }
+  // longest jobs first within each launch
+  for (auto &L : jobs)
+    std::stable_sort(L.begin(), L.end(), [](const SlotJob &a, const SlotJob &b) {
+      return a.last - a.first > b.last - b.first;
+    });
+  // upload and launch the three stages in order on the stream
+  size_t nj = 0, nsv = 0;
+  for (int k = 0; k < 3; k++) { nj += jobs[k].size(); nsv += saves[k].size(); }
+  e = grow<SlotJob>(s.d_jobs, s.jobs_cap, nj);
+  if (e == cudaSuccess) e = grow<SlotSave>(s.d_saves, s.saves_cap, std::max<size_t>(nsv, 1));
+  if (e != cudaSuccess) { s_err = "staged scan job tables: out of device memory"; return HEOM_ERR_NOMEM; }
+  SlotArgs a{};
+  a.N = s.N;
+  a.n_ado = s.n_ado;
+  a.M = s.M;
+  a.K = s.K;
+  a.K_m = s.K_m;
+  a.stride = s.stride;
+  a.wcap = s.sl_wcap;
+  a.ado0 = s.ado0;
+  a.t_start = s.t_start;
+  a.dt = s.dt;
+  for (int q = 0; q < 3; q++) { a.E0[q] = s.E0[q]; a.taup[q] = s.taup[q]; a.w0[q] = s.w0[q]; }
+  a.h = s.h;
+  a.tables = (const unsigned char *)s.d_tables;
+  a.sys = s.d_sys;
+  a.counter = s.d_counter;
+  SlotFn f = slot_kernel(s.precision);
+  size_t jo = 0, so = 0;
+  for (int k = 0; k < 3; k++) {
+    // save indices are relative to the launch's save list
+    if (!jobs[k].empty()) {
+      e = cudaMemcpyAsync((SlotJob *)s.d_jobs + jo, jobs[k].data(), sizeof(SlotJob) * jobs[k].size(),
+                          cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess && !saves[k].empty())
+        e = cudaMemcpyAsync((SlotSave *)s.d_saves + so, saves[k].data(), sizeof(SlotSave) * saves[k].size(),
+                            cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess) e = cudaMemsetAsync(s.d_counter, 0, sizeof(int), st);
+      if (e != cudaSuccess) { s_err = std::string("staged scan upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+      a.jobs = (const SlotJob *)s.d_jobs + jo;
+      a.saves = (const SlotSave *)s.d_saves + so;
+      a.n_jobs = (int)jobs[k].size();
+      const int grid = std::max(1, std::min(a.n_jobs, s.sl_grid));
+      f<<<grid, s.sl_threads, s.sl_smem, st>>>(a);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) { s_err = std::string("staged scan launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+      s.staged_launches++;
+    }
+    jo += jobs[k].size();
+    so += saves[k].size();
+  }
+  return 0;
+}
+
+int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_points, bool tune, cudaStream_t st,
+              bool single_pass) {
   std::vector<unsigned char> tb;
   if (!scan_prepare(s, p, precision, max_points, tb)) return 0; // unsupported: s.why says why
+  if (!single_pass) staged_prepare(s);
   cudaError_t e = cudaMalloc(&s.d_tables, s.tables_bytes);
   if (e == cudaSuccess) e = cudaMemcpy(s.d_tables, tb.data(), s.tables_bytes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMalloc(&s.d_sys, sizeof(double) * sys_doubles(s.N));
@@ -1127,6 +1453,15 @@ int scan_run_device(ScanState &s, const heom_scan_point *d_pts, int n, double *d
                     cudaStream_t st) {
   if (!s.supported) { s_err = "scan path unavailable for this problem: " + s.why; return HEOM_ERR_UNSUPPORTED; }
   if (n == 0) return 0;
+  if (s.staged) { // the stages are planned on the host: read the points back once
+    s.rb_pts.resize(n);
+    s.rb_off.resize(n);
+    cudaError_t e = cudaMemcpyAsync(s.rb_pts.data(), d_pts, sizeof(heom_scan_point) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s.rb_off.data(), d_offsets, sizeof(long long) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { s_err = std::string("scan point read-back: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+    return staged_run(s, s.rb_pts.data(), n, d_P, s.rb_off.data(), st);
+  }
   const void *key[4] = {d_pts, d_P, d_offsets, (const void *)(size_t)(s.variant + 1)};
   if (!s.gexec || s.g_n != n || std::memcmp(key, s.g_key, sizeof key) != 0) {
     if (s.gexec) { cudaGraphExecDestroy(s.gexec); s.gexec = nullptr; }
@@ -1176,7 +1511,7 @@ int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, co
   e = cudaMemcpyAsync(s.d_pts, s.h_pts, sizeof(heom_scan_point) * n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_offsets, s.h_offsets, sizeof(long long) * n, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) { s_err = std::string("scan upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
-  int rc = scan_run_device(s, s.d_pts, n, s.d_P, s.d_offsets, st);
+  int rc = s.staged ? staged_run(s, pts, n, s.d_P, offsets, st) : scan_run_device(s, s.d_pts, n, s.d_P, s.d_offsets, st);
   if (rc) return rc;
   e = cudaMemcpyAsync(s.h_P, s.d_P, sizeof(double2) * total, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -1189,6 +1524,9 @@ int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, co
 
 void scan_release(ScanState &s) {
   if (s.gexec) cudaGraphExecDestroy(s.gexec);
+  if (s.d_snap) cudaFree(s.d_snap);
+  if (s.d_jobs) cudaFree(s.d_jobs);
+  if (s.d_saves) cudaFree(s.d_saves);
   if (s.d_tables) cudaFree(s.d_tables);
   if (s.d_sys) cudaFree(s.d_sys);
   if (s.d_pts) cudaFree(s.d_pts);

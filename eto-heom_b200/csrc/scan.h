@@ -41,13 +41,27 @@ struct ScanState {
   long long *h_offsets = nullptr;
   double *h_P = nullptr;
   long long hP_cap = 0;
+  // staged scan (scan_slots.cuh): shared R/D2 per (tau1, tau2), per-point pulse-3 window,
+  // pulse-free tails two points per CTA
+  bool staged = false;           // chosen for heom_run_scan / heom_run_scan_device
+  bool rstat = false;            // H couples level 0 to nothing (|0><0| stationary)
+  int sl_threads = 0, sl_grid = 0, sl_wcap = 0;
+  size_t sl_smem = 0;
+  void *d_snap = nullptr;        // snapshots: 2 states per regular point
+  size_t snap_cap = 0;
+  void *d_jobs = nullptr, *d_saves = nullptr;
+  size_t jobs_cap = 0, saves_cap = 0;
+  std::vector<heom_scan_point> rb_pts; // points / offsets read back for heom_run_scan_device
+  std::vector<long long> rb_off;
+  long long staged_launches = 0;
   // graph cache for heom_run_scan_device
   cudaGraphExec_t gexec = nullptr;
   const void *g_key[4] = {nullptr, nullptr, nullptr, nullptr};
   int g_n = -1;
 };
 
-int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_points, bool autotune, cudaStream_t st);
+int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_points, bool autotune, cudaStream_t st,
+              bool single_pass = false);
 // Shape + packed tables without any device allocation (false: unsupported, s.why set).
 bool scan_prepare(ScanState &s, const heom::Problem &p, int precision, int max_points,
                   std::vector<unsigned char> &tables);

@@ -1,0 +1,387 @@
+// Staged delay scan: the slot kernel (included by scan.cu after scan_pm.cuh).
+//
+// The single-pass scan kernel propagates, for every point, the four mixed-difference
+// components R, D2, D3, Q from t_start to the point's end.  Points of a scan share most
+// of that work: R depends only on pulse 1's time, D2 only on pulses 1 and 2, and D3 and
+// Q stay exactly zero until pulse 3's window (see scan_pm.cuh); after the last pulse
+// window D2 and D3 no longer feed Q, and R and Q evolve under the pulse-free operator.
+// The staged scan therefore runs three launches of one kernel over "jobs":
+//   1. per group of points with equal (tau1, tau2): R and D2 from t_start up to the last
+//      member's pulse-3 window, saving both states at each member's window start;
+//   2. per point: R, D2, D3, Q through its pulse-3 window from those states (D3 = Q = 0),
+//      recording P and saving R and Q at the window's end;
+//   3. per pair of points: R and Q of each point from those states to the end,
+//      recording P -- two points per CTA, since each needs only two components.
+// Every stage performs the same floating-point operations as the single-pass kernel on
+// the same values, so the results are bit-identical to it.
+//
+// A job holds up to four "slots" (trajectories).  Slot s has an operator (off-diagonal
+// H plus the pulses in its op mask, with the pulse times of its field set), up to two
+// sources -i[V_q, state(src)] (the mixed-difference couplings), an active step range
+// [wake, stop) outside which it keeps its state, and an initial state (zero, |0><0| on
+// ADO 0, or a snapshot).  Layout, thread mapping and stage arithmetic are those of
+// scan_pm (one thread per ADO block of a slot, position-major shared memory, Horner RK4
+// with the FP64 diagonal).
+#pragma once
+
+struct SlotSpec {
+  int op;          // bit q: pulse q+1 enters the operator
+  int fset;        // field set (pulse times) of the operator and the sources
+  int src[2];      // source slots (-1: none)
+  int srcq[2];     // pulse of each source: 1 = pulse 2, 2 = pulse 3
+  int wake, stop;  // active on steps [wake, stop)
+  int init;        // 0: zero, 1: |0><0| on ADO 0, 2: the snapshot at init_ptr
+  int pad;
+  const double2 *init_ptr; // [NN][n_ado], position-major, the kernel's ADO order
+};
+
+struct SlotRec {   // P[rec0 + k] = Tr X3 slot q - Tr X3 slot r at the k-th recorded step
+  int q, r;        // slots (-1: no recorder)
+  int first, last; // steps of the point within the job
+  int rec0, pad;
+  double tau3;
+  double2 *P;      // the point's output
+};
+
+struct SlotJob {
+  int first, last;       // steps [first, last)
+  int save_begin, save_end;
+  double tau[2][3];      // pulse times of the two field sets
+  SlotSpec slot[4];
+  SlotRec rec[2];
+};
+
+struct SlotSave {        // copy slot `slot` before step `step` (step == job.last: after the job)
+  int step, slot;
+  double2 *dst;          // [NN][n_ado]
+};
+
+struct SlotArgs {
+  int N, n_ado, M, K, K_m, n_jobs, stride, wcap, ado0;
+  float t_start, dt;
+  double E0[3], taup[3], w0[3], h;
+  const unsigned char *tables;
+  const double *sys;
+  const SlotJob *jobs;
+  const SlotSave *saves;
+  int *counter;
+};
+
+__device__ __forceinline__ double2 sl_field(const SlotArgs &a, int q, double d) {
+  const double E0 = q == 0 ? a.E0[0] : q == 1 ? a.E0[1] : a.E0[2];
+  const double tp = q == 0 ? a.taup[0] : q == 1 ? a.taup[1] : a.taup[2];
+  const double w0 = q == 0 ? a.w0[0] : q == 1 ? a.w0[1] : a.w0[2];
+  const double Eq = E0 * exp(-2.77 * d * d / tp / tp);
+  double sn, cs;
+  sincos(q == 0 ? w0 * d : -w0 * d, &sn, &cs);
+  return make_double2(Eq * cs, Eq * sn);
+}
+
+template <int NT> __host__ __device__ inline size_t sl_smem_bytes(size_t tsz, int n_ado, int M, int wcap) {
+  constexpr int NN = NT * NT;
+  const size_t nM = (size_t)n_ado * M;
+  const size_t EP = (size_t)NN * pm_stride(n_ado);
+  size_t b = 0;
+  b += al16(16 * EP);                   // rho (FP64)
+  b += al16(2 * 2 * tsz * EP);          // w copies, double-buffered
+  b += al16(2 * tsz * 8 * NN);          // A of 4 slots, V2/V3 of 2 field sets
+  b += al16(16 * (size_t)NN);           // X3
+  b += al16(8 * (size_t)NN);            // Hd[r] - Hd[c]
+  b += al16((tsz == 4 ? 16 : 32) * nM); // links ([o][n])
+  b += al16(16 * (size_t)NN);           // off-diagonal H (FP64)
+  b += al16(16 * 3 * (size_t)NN);       // X0, X1^T, X2^T (FP64)
+  b += al16(16 * (size_t)n_ado);        // damping scalars
+  b += al16(16 * 6 * (size_t)wcap);     // pulse-field windows, 2 field sets x 3 pulses
+  return b;
+}
+
+// One Horner stage of a slot's block: own operator plus up to two sources.
+template <typename T, int NT>
+__device__ __forceinline__ void sl_stage(const PmShared &g, int n, int blk, unsigned am, const typename V2<T>::t *A,
+                                         int sb0, unsigned sm0, const typename V2<T>::t *S0, int sb1, unsigned sm1,
+                                         const typename V2<T>::t *S1, const typename V2<T>::t *__restrict__ W,
+                                         typename V2<T>::t *__restrict__ Wn, const double *__restrict__ Hdd,
+                                         double2 *__restrict__ rho, const PmLink<T> *__restrict__ links, int slot,
+                                         double2 dmp, double cm, bool last, double2 (&w64)[NT * NT]) {
+  using T2 = typename V2<T>::t;
+  const int SP = g.SP, nado = g.nado, K = g.K, Km = g.Km;
+  T kr[NT * NT], ki[NT * NT];
+#pragma unroll
+  for (int e = 0; e < NT * NT; e++) { kr[e] = 0; ki[e] = 0; }
+  if (am) pm_commutator<T, NT, NT, 0>(am, A, W, SP, blk, kr, ki);
+#pragma unroll 1
+  for (int k = 0; k < 2; k++) { // sources -i[V_q, state(src)], the same ADO of another slot
+    const int sb = k == 0 ? sb0 : sb1;
+    const unsigned sm = k == 0 ? sm0 : sm1;
+    if (sb >= 0 && sm) pm_commutator<T, NT, NT, 0>(sm, k == 0 ? S0 : S1, W, SP, sb * nado + n, kr, ki);
+  }
+  const T2 *Wc = W + slot * nado;
+  if (K >= 1) pm_links<T, NT, NT, 0, 1>(Wc, SP, nado, K, Km, n, links, kr, ki);
+  if (NT > 2 && K >= 2) pm_links<T, NT, NT, 0, (NT > 2 ? 2 : 1)>(Wc, SP, nado, K, Km, n, links, kr, ki);
+  if (NT > 3 && K >= 3) pm_links<T, NT, NT, 0, (NT > 3 ? 3 : 1)>(Wc, SP, nado, K, Km, n, links, kr, ki);
+#pragma unroll
+  for (int q = 0; q < NT * NT; q++) {
+    const double gr = dmp.x, gi = dmp.y - Hdd[q];
+    const double2 wv = w64[q];
+    const double k_r = fma(gr, wv.x, fma(-gi, wv.y, (double)kr[q]));
+    const double k_i = fma(gr, wv.y, fma(gi, wv.x, (double)ki[q]));
+    const double2 r0v = rho[q * SP + blk];
+    const double2 wn = make_double2(fma(cm, k_r, r0v.x), fma(cm, k_i, r0v.y));
+    w64[q] = wn;
+    Wn[q * SP + blk] = mk2<T>(wn.x, wn.y);
+    if (last) rho[q * SP + blk] = wn;
+  }
+}
+
+template <typename T, int NT, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
+  using T2 = typename V2<T>::t;
+  constexpr int NN = NT * NT;
+  static_assert(NN <= 32 && NT <= 4, "warp 0 builds A with one lane per element");
+  extern __shared__ __align__(16) unsigned char sm[];
+  __shared__ double2 s_tr[4];
+  __shared__ unsigned s_mask[8];
+  __shared__ int s_lo[6], s_cnt[6], s_job;
+  __shared__ float s_t0;
+  const int M = a.M, nado = a.n_ado, K = a.K, Km = a.K_m, wcap = a.wcap;
+  const int S = 4 * nado, SP = pm_stride(nado);
+  const size_t EP = (size_t)NN * SP;
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const size_t nM = (size_t)nado * M;
+  unsigned char *p = sm;
+  double2 *rho = (double2 *)p;
+  p += al16(16 * EP);
+  T2 *w32 = (T2 *)p; // [2][NN][SP]
+  p += al16(2 * sizeof(T2) * EP);
+  T2 *Aall = (T2 *)p; // [0..3]: slot operators; 4 + 2 f + (q-1): V_{q+1} of field set f
+  p += al16(sizeof(T2) * 8 * NN);
+  double2 *X3 = (double2 *)p;
+  p += al16(16 * (size_t)NN);
+  double *Hdd = (double *)p;
+  p += al16(8 * (size_t)NN);
+  PmLink<T> *links = (PmLink<T> *)p;
+  p += al16(sizeof(PmLink<T>) * nM);
+  double2 *Hoff = (double2 *)p;
+  p += al16(16 * (size_t)NN);
+  double2 *Xf = (double2 *)p; // X0, X1^T, X2^T
+  p += al16(16 * 3 * (size_t)NN);
+  double2 *sdamp = (double2 *)p;
+  p += al16(16 * (size_t)nado);
+  double2 *fwin = (double2 *)p; // [2 field sets][3 pulses][wcap]
+  TableLayout tl(nado, M, Km);
+  const PmLinkHost *g_link = (const PmLinkHost *)(a.tables + tl.plink);
+  const double2 *g_damp = (const double2 *)(a.tables + tl.pdamp);
+  for (size_t q = tid; q < nM; q += bs) {
+    const PmLinkHost L = g_link[q];
+    PmLink<T> v;
+    v.x = (T)L.x;
+    v.by = (T)L.by;
+    v.ay = (T)L.ay;
+    v.ud = L.ud;
+    links[q] = v;
+  }
+  for (int q = tid; q < nado; q += bs) sdamp[q] = g_damp[q];
+  const double *g_Hd = a.sys, *g_Hoff = a.sys + NT, *g_Xs = g_Hoff + 2 * NN, *g_X3 = g_Xs + 6 * NN;
+  for (int q = tid; q < NN; q += bs) {
+    X3[q] = make_double2(g_X3[2 * q], g_X3[2 * q + 1]);
+    Hdd[q] = g_Hd[q / NT] - g_Hd[q % NT];
+    Hoff[q] = make_double2(g_Hoff[2 * q], g_Hoff[2 * q + 1]);
+  }
+  for (int q = tid; q < 3 * NN; q += bs) Xf[q] = make_double2(g_Xs[2 * q], g_Xs[2 * q + 1]);
+  const PmShared gsh{SP, nado, M, K, Km};
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_job = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int jx = s_job;
+    if (jx >= a.n_jobs) break;
+    const SlotJob &J = a.jobs[jx];
+    const int first = J.first, last = J.last;
+    // Pulse windows of both field sets (absolute step indices), and the float time at
+    // step `first`, by the same sequence of roundings as a single-pass run.
+    if (tid < 6) {
+      const int f = tid / 3, q = tid - 3 * f;
+      const double tq = J.tau[f][q];
+      const double tw = 2 * (q == 0 ? a.taup[0] : q == 1 ? a.taup[1] : a.taup[2]);
+      int lo = -1, cnt = 0;
+      float t = a.t_start;
+      for (int i = 0; i < last; i++) {
+        const double d = (double)t - tq;
+        if (fabs(d) <= tw) {
+          if (lo < 0) lo = i;
+          if (cnt < wcap) fwin[(f * 3 + q) * wcap + cnt] = make_double2(d, 0.0);
+          cnt++;
+        } else if (lo >= 0) {
+          break;
+        }
+        t += a.dt;
+      }
+      s_lo[tid] = lo < 0 ? 0 : lo;
+      s_cnt[tid] = cnt;
+    } else if (tid == 6) {
+      float t = a.t_start;
+      for (int i = 0; i < first; i++) t += a.dt;
+      s_t0 = t;
+    }
+    // initial states (both FP32 copies)
+    for (size_t e = tid; e < (size_t)NN * S; e += bs) {
+      const size_t q = e / S, blk = e - q * S;
+      const int sl = (int)(blk / nado), n = (int)(blk - (size_t)sl * nado);
+      const SlotSpec &ss = J.slot[sl];
+      double2 v = make_double2(0.0, 0.0);
+      if (ss.init == 1 && q == 0 && n == a.ado0) v.x = 1.0;
+      else if (ss.init == 2) v = ss.init_ptr[q * nado + n];
+      rho[q * SP + blk] = v;
+      w32[q * SP + blk] = mk2<T>(v.x, v.y);
+      w32[EP + q * SP + blk] = mk2<T>(v.x, v.y);
+    }
+    __syncthreads();
+    for (int w = 0; w < 6; w++) {
+      const int c = min(s_cnt[w], wcap);
+      for (int k = tid; k < c; k += bs)
+        fwin[w * wcap + k] = sl_field(a, w % 3, fwin[w * wcap + k].x);
+    }
+    int lo[6], cn[6];
+#pragma unroll
+    for (int w = 0; w < 6; w++) { lo[w] = s_lo[w]; cn[w] = s_cnt[w]; }
+    // this thread's slot
+    const int sl = tid < S ? tid / nado : -1;
+    const int n = sl >= 0 ? tid - sl * nado : 0;
+    const SlotSpec my = J.slot[sl >= 0 ? sl : 0];
+    const double2 dmp = sl >= 0 ? sdamp[n] : make_double2(0.0, 0.0);
+    int rc0 = 0, rc1 = 0; // records made so far by each recorder
+    int sv = J.save_begin;
+    int buf = 0;
+    float t = s_t0;
+    __syncthreads(); // field tables complete
+    for (int i = first; i <= last; i++) {
+      // snapshots due before step i (after the job at i == last)
+      for (; sv < J.save_end && a.saves[sv].step <= i; sv++) {
+        const SlotSave &s = a.saves[sv];
+        for (size_t e = tid; e < (size_t)NN * nado; e += bs) {
+          const size_t q = e / nado, nn = e - q * nado;
+          s.dst[e] = rho[q * SP + (size_t)s.slot * nado + nn];
+        }
+      }
+      if (i == last) break;
+      bool on[6];
+#pragma unroll
+      for (int w = 0; w < 6; w++) on[w] = (unsigned)(i - lo[w]) < (unsigned)cn[w];
+      bool rec[2];
+#pragma unroll
+      for (int r = 0; r < 2; r++)
+        rec[r] = J.rec[r].q >= 0 && i >= J.rec[r].first && i < J.rec[r].last && t >= J.rec[r].tau3 &&
+                 i % a.stride == 0;
+      if (tid < 32) {
+        // warp 0: the slots' operators, the pulse-2/3 operators of both field sets, their
+        // nonzero masks, and the traces of the recorders' slots (one element per lane)
+        const int q = tid;
+        bool nz[8] = {false, false, false, false, false, false, false, false};
+        double2 c4[4] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0),
+                         make_double2(0.0, 0.0)};
+        if (q < NN) {
+          double vr[6], vi[6];
+#pragma unroll
+          for (int w = 0; w < 6; w++) {
+            double2 ef = make_double2(0.0, 0.0);
+            if (on[w]) {
+              const int k = i - lo[w];
+              ef = cn[w] <= wcap ? fwin[w * wcap + k] : sl_field(a, w % 3, (double)t - J.tau[w / 3][w % 3]);
+            }
+            const double2 x = Xf[(w % 3) * NN + q];
+            vr[w] = -(x.x * ef.x - x.y * ef.y);
+            vi[w] = -(x.x * ef.y + x.y * ef.x);
+          }
+          const double2 h = Hoff[q];
+#pragma unroll
+          for (int s = 0; s < 4; s++) {
+            const int op = J.slot[s].op, f = J.slot[s].fset;
+            double br = h.x, bi = h.y;
+            // the same sums, in the same order, as the single-pass kernel
+            if (op & 1) { br += f ? vr[3] : vr[0]; bi += f ? vi[3] : vi[0]; }
+            if (op & 2) { br += f ? vr[4] : vr[1]; bi += f ? vi[4] : vi[1]; }
+            if (op & 4) { br += f ? vr[5] : vr[2]; bi += f ? vi[5] : vi[2]; }
+            const T2 v = mk2<T>(br, bi);
+            Aall[s * NN + q] = v;
+            nz[s] = v.x != (T)0 || v.y != (T)0;
+          }
+#pragma unroll
+          for (int f = 0; f < 2; f++)
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+              const T2 v = mk2<T>(vr[3 * f + 1 + k], vi[3 * f + 1 + k]);
+              Aall[(4 + 2 * f + k) * NN + q] = v;
+              nz[4 + 2 * f + k] = v.x != (T)0 || v.y != (T)0;
+            }
+#pragma unroll
+          for (int r = 0; r < 2; r++)
+            if (rec[r]) {
+              const int j = q / NT, l = q - j * NT;
+              const double2 x = X3[l * NT + j];
+              const int sq = J.rec[r].q, sr = J.rec[r].r;
+              const double2 z = rho[q * SP + sq * nado + a.ado0];
+              c4[2 * r] = make_double2(z.x * x.x - z.y * x.y, z.x * x.y + z.y * x.x);
+              if (sr >= 0) {
+                const double2 u = rho[q * SP + sr * nado + a.ado0];
+                c4[2 * r + 1] = make_double2(u.x * x.x - u.y * x.y, u.x * x.y + u.y * x.x);
+              }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < 8; s++) {
+          const unsigned b = __ballot_sync(0xffffffffu, nz[s]);
+          if (q == 0) s_mask[s] = b;
+        }
+        if (rec[0] || rec[1]) {
+#pragma unroll
+          for (int o = 16; o >= 1; o >>= 1)
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+              c4[c].x += __shfl_xor_sync(0xffffffffu, c4[c].x, o);
+              c4[c].y += __shfl_xor_sync(0xffffffffu, c4[c].y, o);
+            }
+          if (q == 0)
+#pragma unroll
+            for (int c = 0; c < 4; c++) s_tr[c] = c4[c];
+        }
+      }
+      __syncthreads();
+      if (tid == 0)
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+          if (rec[r]) {
+            const int k = J.rec[r].rec0 + (r == 0 ? rc0 : rc1);
+            J.rec[r].P[k] = make_double2(s_tr[2 * r].x - s_tr[2 * r + 1].x, s_tr[2 * r].y - s_tr[2 * r + 1].y);
+          }
+      rc0 += rec[0];
+      rc1 += rec[1];
+      const bool live = sl >= 0 && i >= my.wake && i < my.stop;
+      const int blk = live ? sl * nado + n : 0;
+      const unsigned am = live ? s_mask[sl] : 0u;
+      // sources whose pulse is on in this slot's field set
+      const int f = my.fset;
+      const bool son0 = live && my.src[0] >= 0 && on[3 * f + my.srcq[0]];
+      const bool son1 = live && my.src[1] >= 0 && on[3 * f + my.srcq[1]];
+      const int sb0 = son0 ? my.src[0] : -1, sb1 = son1 ? my.src[1] : -1;
+      const unsigned sm0 = son0 ? s_mask[4 + 2 * f + my.srcq[0] - 1] : 0u;
+      const unsigned sm1 = son1 ? s_mask[4 + 2 * f + my.srcq[1] - 1] : 0u;
+      const T2 *S0 = Aall + (4 + 2 * f + (son0 ? my.srcq[0] - 1 : 0)) * NN;
+      const T2 *S1 = Aall + (4 + 2 * f + (son1 ? my.srcq[1] - 1 : 0)) * NN;
+      double2 w64[NN];
+#pragma unroll
+      for (int e = 0; e < NN; e++) w64[e] = live ? rho[e * SP + blk] : make_double2(0.0, 0.0);
+      for (int m = 4; m >= 1; m--) {
+        const double cm = a.h / m;
+        const T2 *W = w32 + (size_t)buf * EP;
+        T2 *Wn = w32 + (size_t)(buf ^ 1) * EP;
+        if (live)
+          sl_stage<T, NT>(gsh, n, blk, am, Aall + sl * NN, sb0, sm0, S0, sb1, sm1, S1, W, Wn, Hdd, rho, links, sl,
+                          dmp, cm, m == 1, w64);
+        buf ^= 1;
+        __syncthreads();
+      }
+      t += a.dt;
+    }
+  }
+}

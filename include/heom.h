@@ -109,6 +109,10 @@ typedef struct {
   void *stream;     /* cudaStream_t to run on; NULL = a stream owned by the plan */
   int max_points;   /* capacity of one heom_run_scan call (0 = 1024) */
   int autotune;     /* 1 = time candidate launch shapes at plan creation */
+  int single_pass;  /* 1 = propagate every scan point from t_start in one pass; 0 = stage
+                       the scan (shared R/D2 per (tau1, tau2) group, per-point pulse-3
+                       windows, pulse-free tails two points per CTA) where the problem
+                       allows it -- bit-identical results */
 } heom_opts;
 
 /* Device plan: uploads H, X[0..3], the ADO neighbour tables and the bath
@@ -146,7 +150,9 @@ int heom_scan_layout(const heom_plan *plan, const heom_scan_point *pts, int n,
                      long long *offsets, int *counts, long long *total);
 int heom_run_scan(heom_plan *plan, const heom_scan_point *pts, int n, double *P,
                   const long long *offsets, const int *counts);
-/* Same with every buffer already in device memory; no host synchronisation. */
+/* Same with every buffer already in device memory.  A staged scan reads the points and
+ * offsets back once to plan its stages (one host synchronisation); a single-pass scan
+ * does not synchronise. */
 int heom_run_scan_device(heom_plan *plan, const heom_scan_point *d_pts, int n, double *d_P,
                          const long long *d_offsets);
 
