@@ -1250,61 +1250,93 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     pl[i] = plan_point(s, pts[i]);
     if (pl[i].regular) regular.push_back(i);
   }
-  std::vector<long long> snap_of(n, -1); // first of the point's two snapshot states
-  for (size_t k = 0; k < regular.size(); k++) snap_of[regular[k]] = 2 * (long long)k;
-  cudaError_t e = grow<double2>(s.d_snap, s.snap_cap, std::max<size_t>(2 * regular.size(), 1) * snap_elems);
+  // three states per regular point: R, D2 at its window start; Q - R at its window end
+  std::vector<long long> snap_of(n, -1);
+  for (size_t k = 0; k < regular.size(); k++) snap_of[regular[k]] = 3 * (long long)k;
+  cudaError_t e = grow<double2>(s.d_snap, s.snap_cap, std::max<size_t>(3 * regular.size(), 1) * snap_elems);
+  if (e == cudaSuccess) e = grow<int>(s.d_flags, s.flags_cap, (size_t)n + 1); // + the error word
   if (e != cudaSuccess) { s_err = "staged scan snapshots: out of device memory"; return HEOM_ERR_NOMEM; }
   double2 *snap = (double2 *)s.d_snap;
   auto state = [&](int i, int which) { return snap + (size_t)(snap_of[i] + which) * snap_elems; };
   double2 *P = (double2 *)d_P;
+  auto count_recs = [&](int i, int from, int to) {
+    return records_before(s, pts[i], to) - records_before(s, pts[i], from);
+  };
 
-  std::vector<SlotJob> jobs[3];
-  std::vector<SlotSave> saves[3];
-  // stage 1: R and D2 per (tau1, tau2) group up to the members' pulse-3 windows
+  struct Keyed { long long key; SlotJob job; std::vector<SlotSave> saves; };
+  std::vector<Keyed> q1, q23;
+  // stage 1: R and D2 per (tau1, tau2) group up to the members' pulse-3 windows,
+  // two groups per job
   std::vector<int> order(regular);
   std::sort(order.begin(), order.end(), [&](int a, int b) {
     if (pts[a].tau1 != pts[b].tau1) return pts[a].tau1 < pts[b].tau1;
     if (pts[a].tau2 != pts[b].tau2) return pts[a].tau2 < pts[b].tau2;
     return pl[a].s2 < pl[b].s2;
   });
+  struct Group { int lead, first, last; std::vector<int> members; };
+  std::vector<Group> groups;
   for (size_t g0 = 0; g0 < order.size();) {
     size_t g1 = g0;
     while (g1 < order.size() && pts[order[g1]].tau1 == pts[order[g0]].tau1 &&
            pts[order[g1]].tau2 == pts[order[g0]].tau2)
       g1++;
-    const int lead = order[g0];
-    int last = 0;
-    for (size_t k = g0; k < g1; k++) last = std::max(last, pl[order[k]].s2);
-    const int first = std::min(std::min(pl[lead].wR, pl[lead].wD2), last);
-    SlotJob J{};
-    J.first = first;
-    J.last = last;
-    set_taus(J, 0, pts[lead]);
-    set_taus(J, 1, pts[lead]);
-    J.slot[0] = slot_mk(1, 0, pl[lead].wR, last, 1, nullptr);
-    J.slot[1] = slot_mk(3, 0, pl[lead].wD2, last, 0, nullptr);
-    J.slot[1].src[0] = 0;
-    J.slot[1].srcq[0] = 1;
-    J.slot[2] = J.slot[3] = slot_off();
-    J.rec[0] = J.rec[1] = rec_off();
-    J.save_begin = (int)saves[0].size();
-    for (size_t k = g0; k < g1; k++) { // sorted by s2
-      const int i = order[k];
-      saves[0].push_back(SlotSave{std::max(pl[i].s2, first), 0, state(i, 0)});
-      saves[0].push_back(SlotSave{std::max(pl[i].s2, first), 1, state(i, 1)});
+    Group G;
+    G.lead = order[g0];
+    G.last = 0;
+    for (size_t k = g0; k < g1; k++) {
+      G.members.push_back(order[k]);
+      G.last = std::max(G.last, pl[order[k]].s2);
     }
-    J.save_end = (int)saves[0].size();
-    jobs[0].push_back(J);
+    G.first = std::min(std::min(pl[G.lead].wR, pl[G.lead].wD2), G.last);
+    groups.push_back(G);
     g0 = g1;
+  }
+  std::sort(groups.begin(), groups.end(),
+            [](const Group &a, const Group &b) { return a.last - a.first > b.last - b.first; });
+  for (size_t g = 0; g < groups.size(); g += 2) {
+    Keyed K;
+    SlotJob &J = K.job;
+    J = SlotJob{};
+    J.first = kNever;
+    J.last = 0;
+    J.wait[0] = J.wait[1] = J.wait[2] = J.wait[3] = -1;
+    for (int r = 0; r < 4; r++) J.rec[r] = rec_off();
+    for (int h = 0; h < 2; h++) {
+      J.slot[2 * h] = J.slot[2 * h + 1] = slot_off();
+      if (g + h >= groups.size()) { set_taus(J, h, pts[groups[g].lead]); continue; }
+      const Group &G = groups[g + h];
+      const PtPlan &q = pl[G.lead];
+      set_taus(J, h, pts[G.lead]);
+      J.first = std::min(J.first, G.first);
+      J.last = std::max(J.last, G.last);
+      J.slot[2 * h] = slot_mk(1, h, q.wR, G.last, 1, nullptr);
+      J.slot[2 * h + 1] = slot_mk(3, h, q.wD2, G.last, 0, nullptr);
+      J.slot[2 * h + 1].src[0] = 2 * h;
+      J.slot[2 * h + 1].srcq[0] = 1;
+      for (int i : G.members) {
+        const int st2 = std::max(pl[i].s2, G.first);
+        K.saves.push_back(SlotSave{st2, 2 * h, -1, -1, 0, 0, state(i, 0)});
+        K.saves.push_back(SlotSave{st2, 2 * h + 1, -1, i, 1, 0, state(i, 1)});
+      }
+    }
+    std::stable_sort(K.saves.begin(), K.saves.end(), [](const SlotSave &a, const SlotSave &b) { return a.step < b.step; });
+    for (SlotSave &sv : K.saves) sv.step = std::max(sv.step, J.first);
+    K.key = -1;
+    q1.push_back(std::move(K));
   }
   // stage 2: each point's pulse-3 window (regular points) or the whole point (others)
   for (int i = 0; i < n; i++) {
     const PtPlan &q = pl[i];
     const bool reg = q.regular;
-    SlotJob J{};
+    Keyed K;
+    SlotJob &J = K.job;
+    J = SlotJob{};
     J.first = reg ? q.s2 : 0;
     J.last = reg ? q.s3 : q.nsteps;
-    if (J.last <= J.first && !reg) continue; // an empty point records nothing
+    if (!reg && J.last <= 0) continue; // an empty point records nothing
+    J.wait[0] = reg ? i : -1;
+    J.wait[1] = J.wait[2] = J.wait[3] = -1;
+    J.wait_val = 1;
     set_taus(J, 0, pts[i]);
     set_taus(J, 1, pts[i]);
     J.slot[0] = slot_mk(1, 0, std::max(J.first, q.wR), J.last, reg ? 2 : 1, reg ? state(i, 0) : nullptr);
@@ -1325,61 +1357,77 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     J.rec[0].first = J.first;
     J.rec[0].last = J.last;
     J.rec[0].rec0 = 0;
+    J.rec[0].nrec = count_recs(i, J.first, J.last);
     J.rec[0].tau3 = pts[i].tau3;
     J.rec[0].P = P + offsets[i];
-    J.rec[1] = rec_off();
-    J.save_begin = (int)saves[1].size();
-    if (reg) {
-      saves[1].push_back(SlotSave{J.last, 0, state(i, 0)});
-      saves[1].push_back(SlotSave{J.last, 3, state(i, 1)});
-    }
-    J.save_end = (int)saves[1].size();
-    jobs[1].push_back(J);
+    J.rec[1] = J.rec[2] = J.rec[3] = rec_off();
+    if (reg) K.saves.push_back(SlotSave{J.last, 3, 0, i, 2, 0, state(i, 2)}); // Q - R
+    K.key = reg ? q.s2 : 0;
+    q23.push_back(std::move(K));
   }
-  // stage 3: pulse-free tails of regular points, two per job, paired by window end
+  // stage 3: pulse-free tails D = Q - R of regular points, four per job, grouped by
+  // window end
   std::vector<int> tails;
   for (int i : regular)
     if (pl[i].s3 < pl[i].nsteps) tails.push_back(i);
   std::sort(tails.begin(), tails.end(), [&](int a, int b) {
     return pl[a].s3 != pl[b].s3 ? pl[a].s3 < pl[b].s3 : pl[a].nsteps < pl[b].nsteps;
   });
-  for (size_t k = 0; k < tails.size(); k += 2) {
-    SlotJob J{};
+  for (size_t k = 0; k < tails.size(); k += 4) {
+    Keyed K;
+    SlotJob &J = K.job;
+    J = SlotJob{};
     J.first = kNever;
     J.last = 0;
-    for (int h = 0; h < 2; h++) {
-      J.slot[2 * h] = J.slot[2 * h + 1] = slot_off();
+    J.wait_val = 2;
+    set_taus(J, 0, pts[tails[k]]);
+    set_taus(J, 1, pts[tails[k]]);
+    K.key = 0;
+    for (int h = 0; h < 4; h++) {
+      J.slot[h] = slot_off();
       J.rec[h] = rec_off();
-      if (k + h >= tails.size()) { set_taus(J, h, pts[tails[k]]); continue; }
+      J.wait[h] = -1;
+      if (k + h >= tails.size()) continue;
       const int i = tails[k + h];
       const PtPlan &q = pl[i];
-      set_taus(J, h, pts[i]);
+      J.wait[h] = i;
       J.first = std::min(J.first, q.s3);
       J.last = std::max(J.last, q.nsteps);
-      J.slot[2 * h] = slot_mk(1, h, q.s3, q.nsteps, 2, state(i, 0));
-      J.slot[2 * h + 1] = slot_mk(7, h, q.s3, q.nsteps, 2, state(i, 1));
-      J.rec[h].q = 2 * h + 1;
-      J.rec[h].r = 2 * h;
+      J.slot[h] = slot_mk(0, 0, q.s3, q.nsteps, 2, state(i, 2)); // no pulse is on after s3
+      J.rec[h].q = h;
+      J.rec[h].r = -1;
       J.rec[h].first = q.s3;
       J.rec[h].last = q.nsteps;
       J.rec[h].rec0 = records_before(s, pts[i], q.s3);
+      J.rec[h].nrec = count_recs(i, q.s3, q.nsteps);
       J.rec[h].tau3 = pts[i].tau3;
       J.rec[h].P = P + offsets[i];
+      K.key = std::max<long long>(K.key, q.s3); // ready after the latest window
     }
-    J.save_begin = J.save_end = 0;
-    jobs[2].push_back(J);
+    q23.push_back(std::move(K));
   }
-  // longest jobs first within each launch
-  for (auto &L : jobs)
-    std::stable_sort(L.begin(), L.end(), [](const SlotJob &a, const SlotJob &b) {
-      return a.last - a.first > b.last - b.first;
-    });
-  // upload and launch the three stages in order on the stream
-  size_t nj = 0, nsv = 0;
-  for (int k = 0; k < 3; k++) { nj += jobs[k].size(); nsv += saves[k].size(); }
-  e = grow<SlotJob>(s.d_jobs, s.jobs_cap, nj);
-  if (e == cudaSuccess) e = grow<SlotSave>(s.d_saves, s.saves_cap, std::max<size_t>(nsv, 1));
+  // queue: stage 1 (longest first), then stages 2 and 3 in the order their inputs become
+  // ready (window start for stage 2, window end for stage 3)
+  std::stable_sort(q23.begin(), q23.end(), [](const Keyed &a, const Keyed &b) { return a.key < b.key; });
+  std::vector<SlotJob> jobs;
+  std::vector<SlotSave> saves;
+  for (auto *L : {&q1, &q23})
+    for (Keyed &K : *L) {
+      K.job.save_begin = (int)saves.size();
+      saves.insert(saves.end(), K.saves.begin(), K.saves.end());
+      K.job.save_end = (int)saves.size();
+      jobs.push_back(K.job);
+    }
+  if (jobs.empty()) return 0;
+  e = grow<SlotJob>(s.d_jobs, s.jobs_cap, jobs.size());
+  if (e == cudaSuccess) e = grow<SlotSave>(s.d_saves, s.saves_cap, std::max<size_t>(saves.size(), 1));
   if (e != cudaSuccess) { s_err = "staged scan job tables: out of device memory"; return HEOM_ERR_NOMEM; }
+  e = cudaMemcpyAsync(s.d_jobs, jobs.data(), sizeof(SlotJob) * jobs.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && !saves.empty())
+    e = cudaMemcpyAsync(s.d_saves, saves.data(), sizeof(SlotSave) * saves.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.d_counter, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.d_flags, 0, sizeof(int) * ((size_t)n + 1), st);
+  if (e != cudaSuccess) { s_err = std::string("staged scan upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
   SlotArgs a{};
   a.N = s.N;
   a.n_ado = s.n_ado;
@@ -1396,30 +1444,34 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   a.tables = (const unsigned char *)s.d_tables;
   a.sys = s.d_sys;
   a.counter = s.d_counter;
-  SlotFn f = slot_kernel(s.precision);
-  size_t jo = 0, so = 0;
-  for (int k = 0; k < 3; k++) {
-    // save indices are relative to the launch's save list
-    if (!jobs[k].empty()) {
-      e = cudaMemcpyAsync((SlotJob *)s.d_jobs + jo, jobs[k].data(), sizeof(SlotJob) * jobs[k].size(),
-                          cudaMemcpyHostToDevice, st);
-      if (e == cudaSuccess && !saves[k].empty())
-        e = cudaMemcpyAsync((SlotSave *)s.d_saves + so, saves[k].data(), sizeof(SlotSave) * saves[k].size(),
-                            cudaMemcpyHostToDevice, st);
-      if (e == cudaSuccess) e = cudaMemsetAsync(s.d_counter, 0, sizeof(int), st);
-      if (e != cudaSuccess) { s_err = std::string("staged scan upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
-      a.jobs = (const SlotJob *)s.d_jobs + jo;
-      a.saves = (const SlotSave *)s.d_saves + so;
-      a.n_jobs = (int)jobs[k].size();
-      const int grid = std::max(1, std::min(a.n_jobs, s.sl_grid));
-      f<<<grid, s.sl_threads, s.sl_smem, st>>>(a);
-      e = cudaGetLastError();
-      if (e != cudaSuccess) { s_err = std::string("staged scan launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
-      s.staged_launches++;
-    }
-    jo += jobs[k].size();
-    so += saves[k].size();
-  }
+  a.jobs = (const SlotJob *)s.d_jobs;
+  a.saves = (const SlotSave *)s.d_saves;
+  a.n_jobs = (int)jobs.size();
+  a.flags = (int *)s.d_flags;
+  a.err = (int *)s.d_flags + n;
+  a.wait_ns = 30ull * 1000 * 1000 * 1000; // far above any legitimate wait
+  const int grid = std::max(1, std::min(a.n_jobs, s.sl_grid));
+  slot_kernel(s.precision)<<<grid, s.sl_threads, s.sl_smem, st>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) { s_err = std::string("staged scan launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  s.staged_launches++;
+  s.err_pending = (int *)s.d_flags + n;
+  s.last_work = 0;
+  for (const SlotJob &J : jobs) // propagated component-steps, for the executed-work roofline
+    for (const SlotSpec &z : J.slot) s.last_work += std::max(0, std::min(z.stop, J.last) - std::max(z.wake, J.first));
+  return 0;
+}
+
+// Status of the last staged run once the stream has drained: a dependency wait that gave
+// up leaves HEOM_ERR_TIMEOUT.
+int staged_status(ScanState &s, cudaStream_t st) {
+  if (!s.err_pending) return 0;
+  int err = 0;
+  cudaError_t e = cudaMemcpyAsync(&err, s.err_pending, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) { s_err = std::string("staged scan status: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  s.err_pending = nullptr;
+  if (err) { s_err = "staged scan: a stage waited too long for its inputs"; return HEOM_ERR_TIMEOUT; }
   return 0;
 }
 
@@ -1460,6 +1512,8 @@ int scan_run_device(ScanState &s, const heom_scan_point *d_pts, int n, double *d
     if (e == cudaSuccess) e = cudaMemcpyAsync(s.rb_off.data(), d_offsets, sizeof(long long) * n, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) { s_err = std::string("scan point read-back: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+    int rc = staged_status(s, st); // the previous run, if it has not been checked
+    if (rc) return rc;
     return staged_run(s, s.rb_pts.data(), n, d_P, s.rb_off.data(), st);
   }
   const void *key[4] = {d_pts, d_P, d_offsets, (const void *)(size_t)(s.variant + 1)};
@@ -1516,6 +1570,10 @@ int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, co
   e = cudaMemcpyAsync(s.h_P, s.d_P, sizeof(double2) * total, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) { s_err = std::string("scan run: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  if (s.staged) {
+    rc = staged_status(s, st);
+    if (rc) return rc;
+  }
   std::memcpy(P, s.h_P, sizeof(double2) * total);
   for (long long q = 0; q < 2 * total; q++)
     if (!std::isfinite(P[q])) { s_err = "non-finite P(t) in the scan: the propagation diverged"; return HEOM_ERR_NUMERIC; }
@@ -1525,6 +1583,7 @@ int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, co
 void scan_release(ScanState &s) {
   if (s.gexec) cudaGraphExecDestroy(s.gexec);
   if (s.d_snap) cudaFree(s.d_snap);
+  if (s.d_flags) cudaFree(s.d_flags);
   if (s.d_jobs) cudaFree(s.d_jobs);
   if (s.d_saves) cudaFree(s.d_saves);
   if (s.d_tables) cudaFree(s.d_tables);

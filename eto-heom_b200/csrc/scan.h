@@ -49,8 +49,10 @@ struct ScanState {
   size_t sl_smem = 0;
   void *d_snap = nullptr;        // snapshots: 2 states per regular point
   size_t snap_cap = 0;
-  void *d_jobs = nullptr, *d_saves = nullptr;
-  size_t jobs_cap = 0, saves_cap = 0;
+  void *d_jobs = nullptr, *d_saves = nullptr, *d_flags = nullptr;
+  size_t jobs_cap = 0, saves_cap = 0, flags_cap = 0;
+  int *err_pending = nullptr;    // error word of a run not yet checked
+  long long last_work = 0;       // component-steps propagated by the last staged run
   std::vector<heom_scan_point> rb_pts; // points / offsets read back for heom_run_scan_device
   std::vector<long long> rb_off;
   long long staged_launches = 0;

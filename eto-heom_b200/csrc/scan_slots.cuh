@@ -10,10 +10,21 @@
 //      member's pulse-3 window, saving both states at each member's window start;
 //   2. per point: R, D2, D3, Q through its pulse-3 window from those states (D3 = Q = 0),
 //      recording P and saving R and Q at the window's end;
-//   3. per pair of points: R and Q of each point from those states to the end,
-//      recording P -- two points per CTA, since each needs only two components.
-// Every stage performs the same floating-point operations as the single-pass kernel on
-// the same values, so the results are bit-identical to it.
+//   3. per four points: D = Q - R of each point from the window's end to the point's
+//      end, recording P = Tr X3 D -- four points per CTA.
+// After the last pulse window R and Q evolve under the same pulse-free operator, so
+// their difference D does too, and P = Tr X3 (Q - R) = Tr X3 D: one trajectory per point
+// instead of two.  D is formed in FP64 at the window's end; its FP32 contraction error
+// scales with |D| rather than with |R| and |Q|.  Stages 1 and 2 perform the single-pass
+// kernel's operations on the same values (bit-identical up to the window's end).
+//
+// All three stages run as one persistent launch over a single job queue (stage-1 jobs
+// first, then stage 2, then stage 3).  A job whose inputs come from an earlier job waits
+// on a per-point flag that the producer sets after its snapshot stores are visible.
+// Every producer was dequeued before its consumers, by a CTA that is resident and never
+// waits on a later job, so each wait ends; it is still bounded in time, and a wait that
+// gives up sets an error flag, writes NaN into its outputs and releases its own
+// dependants.
 //
 // A job holds up to four "slots" (trajectories).  Slot s has an operator (off-diagonal
 // H plus the pulses in its op mask, with the pulse times of its field set), up to two
@@ -38,7 +49,7 @@ struct SlotSpec {
 struct SlotRec {   // P[rec0 + k] = Tr X3 slot q - Tr X3 slot r at the k-th recorded step
   int q, r;        // slots (-1: no recorder)
   int first, last; // steps of the point within the job
-  int rec0, pad;
+  int rec0, nrec;  // first record index, records made in [first, last)
   double tau3;
   double2 *P;      // the point's output
 };
@@ -46,13 +57,17 @@ struct SlotRec {   // P[rec0 + k] = Tr X3 slot q - Tr X3 slot r at the k-th reco
 struct SlotJob {
   int first, last;       // steps [first, last)
   int save_begin, save_end;
+  int wait[4], wait_val; // start once flags[wait[k]] >= wait_val (-1: no wait)
+  int pad;
   double tau[2][3];      // pulse times of the two field sets
   SlotSpec slot[4];
-  SlotRec rec[2];
+  SlotRec rec[4];
 };
 
-struct SlotSave {        // copy slot `slot` before step `step` (step == job.last: after the job)
-  int step, slot;
+struct SlotSave {        // copy slot `slot` (minus slot `minus`, unless -1) before step `step`
+  int step, slot, minus; // (step == job.last: after the job)
+  int flag, fval;        // then set flags[flag] = fval (-1: none), once the copy is visible
+  int pad;
   double2 *dst;          // [NN][n_ado]
 };
 
@@ -65,6 +80,9 @@ struct SlotArgs {
   const SlotJob *jobs;
   const SlotSave *saves;
   int *counter;
+  int *flags;            // per-point readiness between stages
+  int *err;              // set to 1 when a dependency wait gives up
+  unsigned long long wait_ns;
 };
 
 __device__ __forceinline__ double2 sl_field(const SlotArgs &a, int q, double d) {
@@ -139,9 +157,9 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
   constexpr int NN = NT * NT;
   static_assert(NN <= 32 && NT <= 4, "warp 0 builds A with one lane per element");
   extern __shared__ __align__(16) unsigned char sm[];
-  __shared__ double2 s_tr[4];
+  __shared__ double2 s_tr[8];
   __shared__ unsigned s_mask[8];
-  __shared__ int s_lo[6], s_cnt[6], s_job;
+  __shared__ int s_lo[6], s_cnt[6], s_job, s_ok;
   __shared__ float s_t0;
   const int M = a.M, nado = a.n_ado, K = a.K, Km = a.K_m, wcap = a.wcap;
   const int S = 4 * nado, SP = pm_stride(nado);
@@ -198,6 +216,37 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
     if (jx >= a.n_jobs) break;
     const SlotJob &J = a.jobs[jx];
     const int first = J.first, last = J.last;
+    if (tid == 0) { // bounded wait for the producers of this job's initial states
+      int ok = 1;
+      if (J.wait[0] >= 0 || J.wait[1] >= 0 || J.wait[2] >= 0 || J.wait[3] >= 0) {
+        unsigned long long t0;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+        for (int k = 0; k < 4 && ok; k++) {
+          if (J.wait[k] < 0) continue;
+          for (;;) {
+            if (atomicAdd(a.flags + J.wait[k], 0) >= J.wait_val) break;
+            unsigned long long t1;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+            if (t1 - t0 > a.wait_ns) { ok = 0; break; }
+            __nanosleep(2000);
+          }
+        }
+        __threadfence();
+      }
+      s_ok = ok;
+    }
+    __syncthreads();
+    if (!s_ok) { // give up: NaN outputs, release dependants, report
+      if (tid == 0) {
+        atomicExch(a.err, 1);
+        const double nan = __longlong_as_double(0x7ff8000000000000LL);
+        for (int r = 0; r < 4; r++)
+          if (J.rec[r].q >= 0 && J.rec[r].nrec > 0) J.rec[r].P[J.rec[r].rec0] = make_double2(nan, nan);
+        for (int k = J.save_begin; k < J.save_end; k++)
+          if (a.saves[k].flag >= 0) atomicMax(a.flags + a.saves[k].flag, a.saves[k].fval);
+      }
+      continue;
+    }
     // Pulse windows of both field sets (absolute step indices), and the float time at
     // step `first`, by the same sequence of roundings as a single-pass run.
     if (tid < 6) {
@@ -231,7 +280,7 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
       const SlotSpec &ss = J.slot[sl];
       double2 v = make_double2(0.0, 0.0);
       if (ss.init == 1 && q == 0 && n == a.ado0) v.x = 1.0;
-      else if (ss.init == 2) v = ss.init_ptr[q * nado + n];
+      else if (ss.init == 2) v = __ldcg(ss.init_ptr + q * nado + n);
       rho[q * SP + blk] = v;
       w32[q * SP + blk] = mk2<T>(v.x, v.y);
       w32[EP + q * SP + blk] = mk2<T>(v.x, v.y);
@@ -250,27 +299,40 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
     const int n = sl >= 0 ? tid - sl * nado : 0;
     const SlotSpec my = J.slot[sl >= 0 ? sl : 0];
     const double2 dmp = sl >= 0 ? sdamp[n] : make_double2(0.0, 0.0);
-    int rc0 = 0, rc1 = 0; // records made so far by each recorder
+    int rcn[4] = {0, 0, 0, 0}; // records made so far by each recorder
     int sv = J.save_begin;
     int buf = 0;
     float t = s_t0;
     __syncthreads(); // field tables complete
     for (int i = first; i <= last; i++) {
       // snapshots due before step i (after the job at i == last)
+      const int sv0 = sv;
       for (; sv < J.save_end && a.saves[sv].step <= i; sv++) {
         const SlotSave &s = a.saves[sv];
         for (size_t e = tid; e < (size_t)NN * nado; e += bs) {
           const size_t q = e / nado, nn = e - q * nado;
-          s.dst[e] = rho[q * SP + (size_t)s.slot * nado + nn];
+          double2 v = rho[q * SP + (size_t)s.slot * nado + nn];
+          if (s.minus >= 0) {
+            const double2 u = rho[q * SP + (size_t)s.minus * nado + nn];
+            v = make_double2(v.x - u.x, v.y - u.y);
+          }
+          __stcg(s.dst + e, v);
         }
+      }
+      if (sv > sv0) { // publish: every thread's stores, then the flags
+        __threadfence();
+        __syncthreads();
+        if (tid == 0)
+          for (int k = sv0; k < sv; k++)
+            if (a.saves[k].flag >= 0) atomicMax(a.flags + a.saves[k].flag, a.saves[k].fval);
       }
       if (i == last) break;
       bool on[6];
 #pragma unroll
       for (int w = 0; w < 6; w++) on[w] = (unsigned)(i - lo[w]) < (unsigned)cn[w];
-      bool rec[2];
+      bool rec[4];
 #pragma unroll
-      for (int r = 0; r < 2; r++)
+      for (int r = 0; r < 4; r++)
         rec[r] = J.rec[r].q >= 0 && i >= J.rec[r].first && i < J.rec[r].last && t >= J.rec[r].tau3 &&
                  i % a.stride == 0;
       if (tid < 32) {
@@ -278,8 +340,9 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
         // nonzero masks, and the traces of the recorders' slots (one element per lane)
         const int q = tid;
         bool nz[8] = {false, false, false, false, false, false, false, false};
-        double2 c4[4] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0),
-                         make_double2(0.0, 0.0)};
+        double2 c4[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) c4[c] = make_double2(0.0, 0.0);
         if (q < NN) {
           double vr[6], vi[6];
 #pragma unroll
@@ -315,7 +378,7 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
               nz[4 + 2 * f + k] = v.x != (T)0 || v.y != (T)0;
             }
 #pragma unroll
-          for (int r = 0; r < 2; r++)
+          for (int r = 0; r < 4; r++)
             if (rec[r]) {
               const int j = q / NT, l = q - j * NT;
               const double2 x = X3[l * NT + j];
@@ -333,29 +396,32 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
           const unsigned b = __ballot_sync(0xffffffffu, nz[s]);
           if (q == 0) s_mask[s] = b;
         }
-        if (rec[0] || rec[1]) {
 #pragma unroll
-          for (int o = 16; o >= 1; o >>= 1)
+        for (int r = 0; r < 4; r++)
+          if (rec[r]) {
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
-              c4[c].x += __shfl_xor_sync(0xffffffffu, c4[c].x, o);
-              c4[c].y += __shfl_xor_sync(0xffffffffu, c4[c].y, o);
+            for (int o = 16; o >= 1; o >>= 1)
+#pragma unroll
+              for (int c = 2 * r; c < 2 * r + 2; c++) {
+                c4[c].x += __shfl_xor_sync(0xffffffffu, c4[c].x, o);
+                c4[c].y += __shfl_xor_sync(0xffffffffu, c4[c].y, o);
+              }
+            if (q == 0) {
+              s_tr[2 * r] = c4[2 * r];
+              s_tr[2 * r + 1] = c4[2 * r + 1];
             }
-          if (q == 0)
-#pragma unroll
-            for (int c = 0; c < 4; c++) s_tr[c] = c4[c];
-        }
+          }
       }
       __syncthreads();
       if (tid == 0)
 #pragma unroll
-        for (int r = 0; r < 2; r++)
+        for (int r = 0; r < 4; r++)
           if (rec[r]) {
-            const int k = J.rec[r].rec0 + (r == 0 ? rc0 : rc1);
+            const int k = J.rec[r].rec0 + rcn[r];
             J.rec[r].P[k] = make_double2(s_tr[2 * r].x - s_tr[2 * r + 1].x, s_tr[2 * r].y - s_tr[2 * r + 1].y);
           }
-      rc0 += rec[0];
-      rc1 += rec[1];
+#pragma unroll
+      for (int r = 0; r < 4; r++) rcn[r] += rec[r];
       const bool live = sl >= 0 && i >= my.wake && i < my.stop;
       const int blk = live ? sl * nado + n : 0;
       const unsigned am = live ? s_mask[sl] : 0u;

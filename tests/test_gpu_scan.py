@@ -104,12 +104,14 @@ def test_scan_device_entry_matches_host_entry(setup):
     assert np.array_equal(dev, host.P)
 
 
-@pytest.mark.parametrize("precision", ["fp32-bulk", "fp64"])
-def test_staged_scan_is_bit_identical_to_single_pass(setup, precision):
-    """The staged scan (shared R/D2 per (tau1, tau2), per-point pulse-3 windows, paired
-    tails) performs the single-pass kernel's operations on the same values.  Includes
-    points that cannot be staged: pulse 3 before pulse 2, pulse 3 outside the point, and
-    an end time inside pulse 3's window."""
+@pytest.mark.parametrize("precision,tol", [("fp32-bulk", FP32_TOL), ("fp64", 1e-11)])
+def test_staged_scan_matches_single_pass(setup, precision, tol):
+    """The staged scan (shared R/D2 per (tau1, tau2), per-point pulse-3 windows, tails
+    D = Q - R four per CTA) against the single pass.  Up to each point's pulse-3 window
+    end it performs the single-pass operations on the same values; the tail propagates
+    Q - R instead of Q and R, which changes rounding only.  Includes points that cannot
+    be staged: pulse 3 before pulse 2, pulse 3 outside the point, an end time inside
+    pulse 3's window."""
     heom, prob = setup
     rows = scan_geometry() + [(50.0, 150.0, 90.0, 260.0), (50.0, 80.0, 400.0, 300.0), (50.0, 70.0, 120.0, 130.0)]
     pts = heom.make_points(rows)
@@ -117,7 +119,9 @@ def test_staged_scan_is_bit_identical_to_single_pass(setup, precision):
     single = heom.Plan(prob, precision, max_points=len(rows), single_pass=True)
     a, b = staged.run_scan(pts), single.run_scan(pts)
     assert np.array_equal(a.counts, b.counts)
-    assert np.array_equal(a.P, b.P), float(np.max(np.abs(a.P - b.P)))
+    errs = [rel_err(a.point(i), b.point(i)) for i in range(len(rows))]
+    print(f"{precision} staged vs single pass: max {max(errs):.2e}")
+    assert max(errs) <= tol
     # the device entry plans the same stages from the points it reads back
     import torch
     lay = staged.scan_layout(pts)
