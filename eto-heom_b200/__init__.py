@@ -103,6 +103,7 @@ def lib() -> ctypes.CDLL:
         "heom_run_scan_device": (I, [P, P, I, P, P]),
         "heom_plan_describe": (I, [P, ctypes.c_char_p, I]),
         "heom_plan_launch_count": (ctypes.c_longlong, [P]),
+        "heom_plan_scan_work": (ctypes.c_longlong, [P]),
         "heom_plan_destroy": (None, [P]),
         "heom_measure_fma_peak": (I, [I, I, D]),
         "heom_run_scan_noalloc": (I, [P, I, P, I, P, P, P]),
@@ -246,6 +247,11 @@ class Plan:
     @property
     def launches(self) -> int:
         return int(lib().heom_plan_launch_count(self._h))
+
+    @property
+    def scan_work(self) -> int:
+        """Component-steps propagated by the last staged scan (0: single pass)."""
+        return int(lib().heom_plan_scan_work(self._h))
 
     def run_traj(self, nv1: int, nv2: int, nv3: int) -> np.ndarray:
         cap = max(self.problem.info.n_record, 1)

@@ -567,6 +567,11 @@ int heom_run_scan_device(heom_plan *pl, const heom_scan_point *d_pts, int n, dou
   return HEOM_OK;
 }
 
+long long heom_plan_scan_work(const heom_plan *pl) {
+  if (!pl) return fail(HEOM_ERR_ARG, "null plan");
+  return pl->scan.staged ? pl->scan.last_work : 0;
+}
+
 int heom_problem_param_count(const heom_problem *h) {
   if (!h) return fail(HEOM_ERR_ARG, "null problem");
   return heom::n_params(h->p);

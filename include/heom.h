@@ -195,6 +195,11 @@ int heom_adjoint_scan(heom_plan *plan, const heom_scan_point *pts, int n, const 
 
 /* Launch shape chosen by the autotuner for this plan ("threads/CTA, CTAs/SM"). */
 int heom_plan_describe(const heom_plan *plan, char *buf, int len);
+/* Component-steps propagated by the plan's last staged delay scan (one component-step =
+ * one RK4 step of one n_ado x N x N state: a reference trajectory step costs the same),
+ * or 0 when the last scan ran in a single pass.  Measurement utility; no counterpart in
+ * the reference. */
+long long heom_plan_scan_work(const heom_plan *plan);
 /* Number of device kernel launches issued by this plan since creation. */
 long long heom_plan_launch_count(const heom_plan *plan);
 void heom_plan_destroy(heom_plan *plan);
