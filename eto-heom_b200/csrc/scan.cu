@@ -1125,26 +1125,44 @@ struct PtPlan {
   bool regular = false;
 };
 
-PtPlan plan_point(const ScanState &s, const heom_scan_point &pt) {
+// The float time grid t_i of the single-pass loop (t_0 = t_start, t_{i+1} = fl(t_i + dt)),
+// shared by every point of a scan; monotone, so window and record bounds are binary
+// searches on it.
+struct TimeGrid {
+  std::vector<float> &t;
+  explicit TimeGrid(std::vector<float> &v) : t(v) {}
+  void ensure(const ScanState &s, int n) { // the grid depends only on t_start and dt
+    if ((int)t.size() >= n) return;
+    t.assign(std::max(n, 1), 0.0f);
+    float x = s.t_start;
+    for (int i = 0; i < n; i++) {
+      t[i] = x;
+      x += s.dt;
+    }
+  }
+  // first i in [0, n) with pred(i) true for a predicate false..false true..true, else n
+  template <class F> static int first_true(int n, F pred) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+      const int mid = lo + (hi - lo) / 2;
+      if (pred(mid)) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+  }
+};
+
+PtPlan plan_point(const ScanState &s, const TimeGrid &g, const heom_scan_point &pt) {
   PtPlan q;
   const float nstep = (pt.t_end - s.t_start) / s.dt;
   q.nsteps = nstep >= 0.0f ? (int)nstep + 1 : 0;
   const double tau[3] = {pt.tau1, pt.tau2, pt.tau3};
-  for (int k = 0; k < 3; k++) {
-    int lo = -1, cnt = 0;
-    float t = s.t_start;
-    for (int i = 0; i < q.nsteps; i++) {
-      const double d = (double)t - tau[k];
-      if (std::fabs(d) <= s.taup[k] * 2) {
-        if (lo < 0) lo = i;
-        cnt++;
-      } else if (lo >= 0) {
-        break;
-      }
-      t += s.dt;
-    }
-    q.lo[k] = lo < 0 ? 0 : lo;
-    q.cnt[k] = cnt;
+  const float *t = g.t.data();
+  for (int k = 0; k < 3; k++) { // steps with |t - tau| <= 2 taup: a contiguous run
+    const double tw = s.taup[k] * 2;
+    const int a = TimeGrid::first_true(q.nsteps, [&](int i) { return (double)t[i] - tau[k] >= -tw; });
+    const int b = TimeGrid::first_true(q.nsteps, [&](int i) { return (double)t[i] - tau[k] > tw; });
+    q.lo[k] = a < b ? a : 0;
+    q.cnt[k] = a < b ? b - a : 0;
   }
   q.wR = s.rstat ? (q.cnt[0] > 0 ? q.lo[0] : kNever) : 0;
   q.wD2 = q.cnt[1] > 0 ? q.lo[1] : kNever;
@@ -1155,26 +1173,19 @@ PtPlan plan_point(const ScanState &s, const heom_scan_point &pt) {
   q.s2 = std::min(q.wD3, q.wQ);
   for (int k = 0; k < 3; k++)
     if (q.cnt[k] > 0) q.s3 = std::max(q.s3, q.lo[k] + q.cnt[k]);
-  q.rs = q.nsteps;
-  float t = s.t_start;
-  for (int i = 0; i < q.nsteps; i++) {
-    if (t >= pt.tau3 && i % s.stride == 0) { q.rs = i; break; }
-    t += s.dt;
-  }
+  // first record: the first multiple of the stride at or after the first t >= tau3
+  const int i3 = TimeGrid::first_true(q.nsteps, [&](int i) { return t[i] >= pt.tau3; });
+  q.rs = i3 >= q.nsteps ? q.nsteps : std::min(q.nsteps, (i3 + s.stride - 1) / s.stride * s.stride);
   // Stageable: D3 and Q wake inside the point, no P record before they do, and every
   // pulse window closes inside the point.
   q.regular = q.s2 < q.nsteps && q.s2 <= q.s3 && q.s3 <= q.nsteps && q.rs >= q.s2;
   return q;
 }
 
-int records_before(const ScanState &s, const heom_scan_point &pt, int upto) {
-  int c = 0;
-  float t = s.t_start;
-  for (int i = 0; i < upto; i++) {
-    if (t >= pt.tau3 && i % s.stride == 0) c++;
-    t += s.dt;
-  }
-  return c;
+// Records of a point in steps [0, upto): every stride-th step from its first record on.
+int records_before(const ScanState &s, const PtPlan &q, int upto) {
+  upto = std::min(upto, q.nsteps);
+  return upto <= q.rs ? 0 : (upto - q.rs + s.stride - 1) / s.stride;
 }
 
 SlotSpec slot_off() {
@@ -1246,8 +1257,17 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   const size_t snap_elems = (size_t)NN * s.n_ado; // double2 per state
   std::vector<PtPlan> pl(n);
   std::vector<int> regular;
+  {
+    int maxsteps = 0;
+    for (int i = 0; i < n; i++) {
+      const float nstep = (pts[i].t_end - s.t_start) / s.dt;
+      maxsteps = std::max(maxsteps, nstep >= 0.0f ? (int)nstep + 1 : 0);
+    }
+    TimeGrid(s.t_grid).ensure(s, maxsteps);
+  }
+  const TimeGrid tgrid(s.t_grid);
   for (int i = 0; i < n; i++) {
-    pl[i] = plan_point(s, pts[i]);
+    pl[i] = plan_point(s, tgrid, pts[i]);
     if (pl[i].regular) regular.push_back(i);
   }
   // three states per regular point: R, D2 at its window start; Q - R at its window end
@@ -1260,7 +1280,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   auto state = [&](int i, int which) { return snap + (size_t)(snap_of[i] + which) * snap_elems; };
   double2 *P = (double2 *)d_P;
   auto count_recs = [&](int i, int from, int to) {
-    return records_before(s, pts[i], to) - records_before(s, pts[i], from);
+    return records_before(s, pl[i], to) - records_before(s, pl[i], from);
   };
 
   struct Keyed { long long key; SlotJob job; std::vector<SlotSave> saves; };
@@ -1398,7 +1418,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       J.rec[h].r = -1;
       J.rec[h].first = q.s3;
       J.rec[h].last = q.nsteps;
-      J.rec[h].rec0 = records_before(s, pts[i], q.s3);
+      J.rec[h].rec0 = records_before(s, q, q.s3);
       J.rec[h].nrec = count_recs(i, q.s3, q.nsteps);
       J.rec[h].tau3 = pts[i].tau3;
       J.rec[h].P = P + offsets[i];

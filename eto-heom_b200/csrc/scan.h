@@ -53,6 +53,7 @@ struct ScanState {
   size_t jobs_cap = 0, saves_cap = 0, flags_cap = 0;
   int *err_pending = nullptr;    // error word of a run not yet checked
   long long last_work = 0;       // component-steps propagated by the last staged run
+  std::vector<float> t_grid;     // float time of each step (t_start + dt accumulated)
   std::vector<heom_scan_point> rb_pts; // points / offsets read back for heom_run_scan_device
   std::vector<long long> rb_off;
   long long staged_launches = 0;
