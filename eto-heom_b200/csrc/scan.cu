@@ -890,10 +890,60 @@ cudaError_t scan_enqueue(const ScanState &s, const heom_scan_point *d_pts, int n
   return enqueue(s, d_pts, n, d_P, d_offsets, st);
 }
 
+// Reduced-tail table of the current sample: the positions P reads (X3[l][j] != 0 reads
+// element (j, l)), closed under the off-diagonal H, and the commutator with H restricted
+// to them (see scan_slots.cuh).  n = 0 when the closure exceeds kTailMax positions.
+static void tail_table(const std::vector<double> &sys, int N, std::vector<double> &tab) {
+  const int NN = N * N;
+  const double *Hoff = sys.data() + N, *X3 = Hoff + 2 * NN + 6 * NN;
+  auto nz = [](const double *m, int i) { return m[2 * i] != 0.0 || m[2 * i + 1] != 0.0; };
+  std::vector<char> in(NN, 0);
+  for (int j = 0; j < N; j++)
+    for (int l = 0; l < N; l++)
+      if (nz(X3, l * N + j)) in[j * N + l] = 1;
+  for (bool changed = true; changed;) {
+    changed = false;
+    for (int q = 0; q < NN; q++) {
+      if (!in[q]) continue;
+      const int r = q / N, c = q % N;
+      for (int l = 0; l < N; l++) {
+        if (l != r && nz(Hoff, r * N + l) && !in[l * N + c]) { in[l * N + c] = 1; changed = true; }
+        if (l != c && nz(Hoff, l * N + c) && !in[r * N + l]) { in[r * N + l] = 1; changed = true; }
+      }
+    }
+  }
+  std::vector<int> pos;
+  for (int q = 0; q < NN; q++)
+    if (in[q]) pos.push_back(q);
+  tab.assign(tail_doubles(), 0.0);
+  if (pos.empty() || (int)pos.size() > kTailMax) return;
+  tab[0] = (double)pos.size();
+  double *C = tab.data() + 1 + kTailMax;
+  for (size_t e = 0; e < pos.size(); e++) {
+    tab[1 + e] = pos[e];
+    const int r = pos[e] / N, c = pos[e] % N;
+    for (size_t f = 0; f < pos.size(); f++) {
+      const int l = pos[f] / N, c2 = pos[f] % N;
+      double cr = 0.0, ci = 0.0;
+      if (c2 == c) { cr += Hoff[2 * (r * N + l)]; ci += Hoff[2 * (r * N + l) + 1]; }   // (H w)[r][c]
+      if (l == r) { cr -= Hoff[2 * (c2 * N + c)]; ci -= Hoff[2 * (c2 * N + c) + 1]; } // (w H)[r][c]
+      C[2 * (e * kTailMax + f)] = cr;
+      C[2 * (e * kTailMax + f) + 1] = ci;
+    }
+  }
+}
+
 int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
   if (!s.supported) return 0;
   std::vector<double> sys;
   scan_system_host(p, sys);
+  if (s.staged && s.d_tail) {
+    std::vector<double> tab;
+    tail_table(sys, s.N, tab);
+    s.tail_n = (int)tab[0];
+    cudaError_t e = cudaMemcpyAsync(s.d_tail, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) { s_err = std::string("tail table upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  }
   { // the kernels' test for a stationary |0><0| (off-diagonal H in row and column 0)
     const double *Hoff = sys.data() + s.N;
     bool z = true;
@@ -1400,6 +1450,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     J.first = kNever;
     J.last = 0;
     J.wait_val = 2;
+    J.mode = s.tail_n > 0 ? 1 : 0; // reduced positions when the sample allows it
     set_taus(J, 0, pts[tails[k]]);
     set_taus(J, 1, pts[tails[k]]);
     K.key = 0;
@@ -1470,6 +1521,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   a.flags = (int *)s.d_flags;
   a.err = (int *)s.d_flags + n;
   a.wait_ns = 30ull * 1000 * 1000 * 1000; // far above any legitimate wait
+  a.tail = s.tail_n > 0 ? (const double *)s.d_tail : nullptr;
   const int grid = std::max(1, std::min(a.n_jobs, s.sl_grid));
   slot_kernel(s.precision)<<<grid, s.sl_threads, s.sl_smem, st>>>(a);
   e = cudaGetLastError();
@@ -1477,8 +1529,11 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   s.staged_launches++;
   s.err_pending = (int *)s.d_flags + n;
   s.last_work = 0;
-  for (const SlotJob &J : jobs) // propagated component-steps, for the executed-work roofline
-    for (const SlotSpec &z : J.slot) s.last_work += std::max(0, std::min(z.stop, J.last) - std::max(z.wake, J.first));
+  for (const SlotJob &J : jobs) { // propagated component-steps (a reduced step counts its share)
+    long long w = 0;
+    for (const SlotSpec &z : J.slot) w += std::max(0, std::min(z.stop, J.last) - std::max(z.wake, J.first));
+    s.last_work += J.mode == 1 ? w * s.tail_n / (s.N * s.N) : w;
+  }
   return 0;
 }
 
@@ -1509,6 +1564,7 @@ int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_point
   if (e == cudaSuccess) e = cudaMalloc(&s.d_counter, sizeof(int) * 4);
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_pts, sizeof(heom_scan_point) * max_points);
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_offsets, sizeof(long long) * max_points);
+  if (e == cudaSuccess && s.staged) e = cudaMalloc(&s.d_tail, sizeof(double) * tail_doubles());
   if (e != cudaSuccess) { s_err = std::string("scan buffers: ") + cudaGetErrorString(e); return HEOM_ERR_NOMEM; }
   s.supported = true;
   int rc = scan_upload_system(s, p, st);
@@ -1604,6 +1660,7 @@ void scan_release(ScanState &s) {
   if (s.gexec) cudaGraphExecDestroy(s.gexec);
   if (s.d_snap) cudaFree(s.d_snap);
   if (s.d_flags) cudaFree(s.d_flags);
+  if (s.d_tail) cudaFree(s.d_tail);
   if (s.d_jobs) cudaFree(s.d_jobs);
   if (s.d_saves) cudaFree(s.d_saves);
   if (s.d_tables) cudaFree(s.d_tables);

@@ -54,6 +54,8 @@ struct ScanState {
   int *err_pending = nullptr;    // error word of a run not yet checked
   long long last_work = 0;       // component-steps propagated by the last staged run
   std::vector<float> t_grid;     // float time of each step (t_start + dt accumulated)
+  void *d_tail = nullptr;        // reduced-tail table of the current sample
+  int tail_n = 0;                // its positions (0: tails run on full blocks)
   std::vector<heom_scan_point> rb_pts; // points / offsets read back for heom_run_scan_device
   std::vector<long long> rb_off;
   long long staged_launches = 0;

@@ -18,6 +18,13 @@
 // scales with |D| rather than with |R| and |Q|.  Stages 1 and 2 perform the single-pass
 // kernel's operations on the same values (bit-identical up to the window's end).
 //
+// Reduced tails.  With every pulse off, H (block-diagonal in excitation number) and the
+// bath (site projectors) map each element position of an ADO block to positions coupled
+// by the off-diagonal H only.  P reads the positions where X3 is nonzero; the closure of
+// that set under the off-diagonal H (computed on the host per sample, at most kTailMax
+// positions) evolves on its own.  Tail jobs in reduced mode propagate only those
+// positions: 4 of 16 for the dimer (the (singles, ground) and (doubles, singles) blocks).
+//
 // All three stages run as one persistent launch over a single job queue (stage-1 jobs
 // first, then stage 2, then stage 3).  A job whose inputs come from an earlier job waits
 // on a per-point flag that the producer sets after its snapshot stores are visible.
@@ -58,7 +65,7 @@ struct SlotJob {
   int first, last;       // steps [first, last)
   int save_begin, save_end;
   int wait[4], wait_val; // start once flags[wait[k]] >= wait_val (-1: no wait)
-  int pad;
+  int mode;              // 0: full blocks; 1: the reduced tail positions only
   double tau[2][3];      // pulse times of the two field sets
   SlotSpec slot[4];
   SlotRec rec[4];
@@ -83,7 +90,14 @@ struct SlotArgs {
   int *flags;            // per-point readiness between stages
   int *err;              // set to 1 when a dependency wait gives up
   unsigned long long wait_ns;
+  const double *tail;    // [n][pos x kTailMax][C: kTailMax x kTailMax complex], see tail_table
 };
+
+constexpr int kTailMax = 8;
+// Reduced-tail table (doubles): [0] = n positions (0: none), [1..kTailMax] = positions
+// r*N + c, then C (kTailMax x kTailMax complex, row-major): X_e = sum_e' C[e][e'] w_e' is
+// the commutator [H_off, w] restricted to the positions.
+__host__ __device__ inline size_t tail_doubles() { return 1 + kTailMax + 2 * kTailMax * kTailMax; }
 
 __device__ __forceinline__ double2 sl_field(const SlotArgs &a, int q, double d) {
   const double E0 = q == 0 ? a.E0[0] : q == 1 ? a.E0[1] : a.E0[2];
@@ -151,6 +165,91 @@ __device__ __forceinline__ void sl_stage(const PmShared &g, int n, int blk, unsi
   }
 }
 
+// One Horner stage of the reduced tail: positions tpos[0..ne) of the slot's block.
+template <typename T, int NT>
+__device__ __forceinline__ void sl_stage_tail(const PmShared &g, int n, int blk, int slot, int ne,
+                                              const int *__restrict__ tpos, const unsigned *__restrict__ tmask,
+                                              const typename V2<T>::t *__restrict__ tC,
+                                              const typename V2<T>::t *__restrict__ W,
+                                              typename V2<T>::t *__restrict__ Wn, const double *__restrict__ Hdd,
+                                              double2 *__restrict__ rho, const PmLink<T> *__restrict__ links,
+                                              double2 dmp, double cm, bool last, double2 (&w64)[NT * NT]) {
+  using T2 = typename V2<T>::t;
+  const int SP = g.SP, nado = g.nado, K = g.K, Km = g.Km;
+  T kr[kTailMax], ki[kTailMax];
+  T2 zb[kTailMax];
+#pragma unroll
+  for (int e = 0; e < kTailMax; e++) {
+    kr[e] = 0;
+    ki[e] = 0;
+    zb[e] = e < ne ? W[tpos[e] * SP + blk] : mk2<T>(0.0, 0.0);
+  }
+#pragma unroll
+  for (int e = 0; e < kTailMax; e++) { // X = C z, k = -i X
+    if (e >= ne) break;
+#pragma unroll
+    for (int f = 0; f < kTailMax; f++) {
+      if (!(tmask[e] & (1u << f))) continue;
+      const T2 a = tC[e * kTailMax + f], z = zb[f];
+      ki[e] = fma(-a.x, z.x, ki[e]);
+      ki[e] = fma(a.y, z.y, ki[e]);
+      kr[e] = fma(a.x, z.y, kr[e]);
+      kr[e] = fma(a.y, z.x, kr[e]);
+    }
+  }
+  const T2 *Wc = W + slot * nado;
+#pragma unroll
+  for (int e = 0; e < kTailMax; e++) { // bath links of site levels r (row) and c (column)
+    if (e >= ne) break;
+    const int q = tpos[e], r = q / NT, c = q - r * NT;
+    if (r >= 1 && r <= K)
+      for (int k = 0; k < Km; k++) {
+        const PmLink<T> L = links[((r - 1) + k * K) * nado + n];
+        const unsigned u = (unsigned)L.ud & 0xffffu, d = (unsigned)L.ud >> 16;
+        if (u != 0xffffu && c != r) { // row r: +i x w_u
+          const T2 z = Wc[q * SP + u];
+          kr[e] = fma(-L.x, z.y, kr[e]);
+          ki[e] = fma(L.x, z.x, ki[e]);
+        }
+        if (d != 0xffffu) { // row r: (-b y, a y) w_d; diagonal (-2 b y, 0)
+          const T2 z = Wc[q * SP + d];
+          const T cr = c == r ? -2 * L.by : -L.by, ci = c == r ? (T)0 : L.ay;
+          kr[e] = fma(cr, z.x, fma(-ci, z.y, kr[e]));
+          ki[e] = fma(cr, z.y, fma(ci, z.x, ki[e]));
+        }
+      }
+    if (c >= 1 && c <= K && c != r)
+      for (int k = 0; k < Km; k++) {
+        const PmLink<T> L = links[((c - 1) + k * K) * nado + n];
+        const unsigned u = (unsigned)L.ud & 0xffffu, d = (unsigned)L.ud >> 16;
+        if (u != 0xffffu) { // column c: -i x w_u
+          const T2 z = Wc[q * SP + u];
+          kr[e] = fma(L.x, z.y, kr[e]);
+          ki[e] = fma(-L.x, z.x, ki[e]);
+        }
+        if (d != 0xffffu) { // column c: (-b y, -a y) w_d
+          const T2 z = Wc[q * SP + d];
+          kr[e] = fma(-L.by, z.x, fma(L.ay, z.y, kr[e]));
+          ki[e] = fma(-L.by, z.y, fma(-L.ay, z.x, ki[e]));
+        }
+      }
+  }
+#pragma unroll
+  for (int e = 0; e < kTailMax; e++) {
+    if (e >= ne) break;
+    const int q = tpos[e];
+    const double gr = dmp.x, gi = dmp.y - Hdd[q];
+    const double2 wv = w64[e];
+    const double k_r = fma(gr, wv.x, fma(-gi, wv.y, (double)kr[e]));
+    const double k_i = fma(gr, wv.y, fma(gi, wv.x, (double)ki[e]));
+    const double2 r0v = rho[q * SP + blk];
+    const double2 wn = make_double2(fma(cm, k_r, r0v.x), fma(cm, k_i, r0v.y));
+    w64[e] = wn;
+    Wn[q * SP + blk] = mk2<T>(wn.x, wn.y);
+    if (last) rho[q * SP + blk] = wn;
+  }
+}
+
 template <typename T, int NT, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
   using T2 = typename V2<T>::t;
@@ -159,6 +258,9 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
   extern __shared__ __align__(16) unsigned char sm[];
   __shared__ double2 s_tr[8];
   __shared__ unsigned s_mask[8];
+  __shared__ int s_tpos[kTailMax], s_tn;
+  __shared__ unsigned s_tmask[kTailMax];
+  __shared__ typename V2<T>::t s_tC[kTailMax * kTailMax];
   __shared__ int s_lo[6], s_cnt[6], s_job, s_ok;
   __shared__ float s_t0;
   const int M = a.M, nado = a.n_ado, K = a.K, Km = a.K_m, wcap = a.wcap;
@@ -206,6 +308,18 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
     Hoff[q] = make_double2(g_Hoff[2 * q], g_Hoff[2 * q + 1]);
   }
   for (int q = tid; q < 3 * NN; q += bs) Xf[q] = make_double2(g_Xs[2 * q], g_Xs[2 * q + 1]);
+  if (tid == 0) s_tn = a.tail ? (int)a.tail[0] : 0;
+  if (tid < kTailMax) {
+    s_tpos[tid] = a.tail ? (int)a.tail[1 + tid] : 0;
+    unsigned m = 0;
+    for (int f = 0; f < kTailMax; f++) {
+      const double cr = a.tail ? a.tail[1 + kTailMax + 2 * (tid * kTailMax + f)] : 0.0;
+      const double ci = a.tail ? a.tail[1 + kTailMax + 2 * (tid * kTailMax + f) + 1] : 0.0;
+      s_tC[tid * kTailMax + f] = mk2<T>(cr, ci);
+      if (cr != 0.0 || ci != 0.0) m |= 1u << f;
+    }
+    s_tmask[tid] = m;
+  }
   const PmShared gsh{SP, nado, M, K, Km};
 
   for (;;) {
@@ -435,13 +549,23 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
       const T2 *S0 = Aall + (4 + 2 * f + (son0 ? my.srcq[0] - 1 : 0)) * NN;
       const T2 *S1 = Aall + (4 + 2 * f + (son1 ? my.srcq[1] - 1 : 0)) * NN;
       double2 w64[NN];
+      if (J.mode == 1) { // reduced tail: w64[e] is position s_tpos[e]
 #pragma unroll
-      for (int e = 0; e < NN; e++) w64[e] = live ? rho[e * SP + blk] : make_double2(0.0, 0.0);
+        for (int e = 0; e < NN; e++)
+          w64[e] = (live && e < kTailMax && e < s_tn) ? rho[s_tpos[e < kTailMax ? e : 0] * SP + blk]
+                                                      : make_double2(0.0, 0.0);
+      } else {
+#pragma unroll
+        for (int e = 0; e < NN; e++) w64[e] = live ? rho[e * SP + blk] : make_double2(0.0, 0.0);
+      }
       for (int m = 4; m >= 1; m--) {
         const double cm = a.h / m;
         const T2 *W = w32 + (size_t)buf * EP;
         T2 *Wn = w32 + (size_t)(buf ^ 1) * EP;
-        if (live)
+        if (live && J.mode == 1)
+          sl_stage_tail<T, NT>(gsh, n, blk, sl, s_tn, s_tpos, s_tmask, s_tC, W, Wn, Hdd, rho, links, dmp, cm,
+                               m == 1, w64);
+        else if (live)
           sl_stage<T, NT>(gsh, n, blk, am, Aall + sl * NN, sb0, sm0, S0, sb1, sm1, S1, W, Wn, Hdd, rho, links, sl,
                           dmp, cm, m == 1, w64);
         buf ^= 1;
