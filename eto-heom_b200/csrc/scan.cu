@@ -1443,7 +1443,8 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   std::sort(tails.begin(), tails.end(), [&](int a, int b) {
     return pl[a].s3 != pl[b].s3 ? pl[a].s3 < pl[b].s3 : pl[a].nsteps < pl[b].nsteps;
   });
-  for (size_t k = 0; k < tails.size(); k += 4) {
+  const bool tail_kernel = s.tail_n > 0;
+  for (size_t k = 0; k < (tail_kernel ? 0 : tails.size()); k += 4) {
     Keyed K;
     SlotJob &J = K.job;
     J = SlotJob{};
@@ -1528,12 +1529,74 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   if (e != cudaSuccess) { s_err = std::string("staged scan launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
   s.staged_launches++;
   s.err_pending = (int *)s.d_flags + n;
+  long long tail_work = 0;
+  if (tail_kernel && !tails.empty()) {
+    // G points per CTA on the reduced positions, at least one CTA per SM when possible
+    const int per_cta = std::max(1, kTailThreads / s.n_ado);
+    const int G = std::max(1, std::min(per_cta, (int)((tails.size() + s.sm_count - 1) / s.sm_count)));
+    const int nblk = (int)((tails.size() + G - 1) / G);
+    std::vector<TailPoint> tp(tails.size());
+    std::vector<float> tfirst(nblk);
+    for (size_t k = 0; k < tails.size(); k++) {
+      const int i = tails[k];
+      const PtPlan &q = pl[i];
+      TailPoint &T = tp[k];
+      T.first = q.s3;
+      T.last = q.nsteps;
+      T.rec0 = records_before(s, q, q.s3);
+      T.pad = 0;
+      T.tau3 = pts[i].tau3;
+      T.init = state(i, 2);
+      T.P = P + offsets[i];
+      tail_work += q.nsteps - q.s3;
+    }
+    for (int b = 0; b < nblk; b++) {
+      int f = kNever;
+      for (int k = b * G; k < std::min((int)tails.size(), (b + 1) * G); k++) f = std::min(f, tp[k].first);
+      tfirst[b] = s.t_grid[f];
+    }
+    e = grow<TailPoint>(s.d_tailpts, s.tailpts_cap, tp.size());
+    if (e == cudaSuccess) e = grow<float>(s.d_tfirst, s.tfirst_cap, tfirst.size());
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s.d_tailpts, tp.data(), sizeof(TailPoint) * tp.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s.d_tfirst, tfirst.data(), sizeof(float) * tfirst.size(), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) { s_err = std::string("tail upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+    TailArgs ta{};
+    ta.N = s.N;
+    ta.n_ado = s.n_ado;
+    ta.M = s.M;
+    ta.K = s.K;
+    ta.K_m = s.K_m;
+    ta.stride = s.stride;
+    ta.ado0 = s.ado0;
+    ta.n_pts = (int)tp.size();
+    ta.G = G;
+    ta.dt = s.dt;
+    ta.h = s.h;
+    ta.tables = (const unsigned char *)s.d_tables;
+    ta.sys = s.d_sys;
+    ta.tail = (const double *)s.d_tail;
+    ta.pts = (const TailPoint *)s.d_tailpts;
+    ta.t_first = (const float *)s.d_tfirst;
+    const size_t tsz = s.precision == HEOM_FP64 ? 8 : 4;
+    const size_t smem = tail_smem_bytes<4>(tsz, s.n_ado, s.M, G, s.tail_n);
+    auto tk = s.precision == HEOM_FP64 ? scan_tail<double, 4> : scan_tail<float, 4>;
+    e = cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) {
+      tk<<<nblk, (G * s.n_ado + 31) / 32 * 32, smem, st>>>(ta);
+      e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) { s_err = std::string("tail launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+    s.staged_launches++;
+  }
   s.last_work = 0;
   for (const SlotJob &J : jobs) { // propagated component-steps (a reduced step counts its share)
     long long w = 0;
     for (const SlotSpec &z : J.slot) w += std::max(0, std::min(z.stop, J.last) - std::max(z.wake, J.first));
     s.last_work += J.mode == 1 ? w * s.tail_n / (s.N * s.N) : w;
   }
+  s.last_work += tail_work * s.tail_n / (s.N * s.N);
   return 0;
 }
 
@@ -1661,6 +1724,8 @@ void scan_release(ScanState &s) {
   if (s.d_snap) cudaFree(s.d_snap);
   if (s.d_flags) cudaFree(s.d_flags);
   if (s.d_tail) cudaFree(s.d_tail);
+  if (s.d_tailpts) cudaFree(s.d_tailpts);
+  if (s.d_tfirst) cudaFree(s.d_tfirst);
   if (s.d_jobs) cudaFree(s.d_jobs);
   if (s.d_saves) cudaFree(s.d_saves);
   if (s.d_tables) cudaFree(s.d_tables);

@@ -56,6 +56,8 @@ struct ScanState {
   std::vector<float> t_grid;     // float time of each step (t_start + dt accumulated)
   void *d_tail = nullptr;        // reduced-tail table of the current sample
   int tail_n = 0;                // its positions (0: tails run on full blocks)
+  void *d_tailpts = nullptr, *d_tfirst = nullptr; // the tail kernel's points and start times
+  size_t tailpts_cap = 0, tfirst_cap = 0;
   std::vector<heom_scan_point> rb_pts; // points / offsets read back for heom_run_scan_device
   std::vector<long long> rb_off;
   long long staged_launches = 0;
