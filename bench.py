@@ -364,13 +364,39 @@ def run_ours(a):
 
 
 def profile_run(precision: str):
-    """A small case of the same kernel for profiler captures: the first 148 points of
-    the scan (one per SM) with t3 shortened to 50 fs, default launch shape, one run."""
+    """A small case of a kernel for profiler captures.
+
+    fp32-bulk / fp64: the first 148 points of the dimer scan (one per SM) with t3
+    shortened to 50 fs, default launch shape, one run of the scan kernel.
+    c1-*: one 2DES point of the FMO key (N = 8, 680 ADOs) with the pulses at 10, 20 and
+    30 fs (5 fs wide) and the end at 40 fs -- 81 RK4 steps of the general-size staged
+    path (c1-fp32-bulk, c1-fp64) or of the bit-exact path (c1-fp64-exact)."""
     import torch
 
     from heomtest import load_pkg
 
     heom = load_pkg()
+    if precision.startswith("c1-"):
+        with open(os.path.join(ROOT, "tests", "golden", "keys", "c1_fmo.key")) as f:
+            text = f.read()
+        pulses = "PULSE\n3\n0.5308 50 20 12500\n0.5308 150 20 12500\n0.5308 250 20 12500"
+        assert pulses in text and "TIME\n0 2000 0.5 0.5" in text
+        text = text.replace(pulses, "PULSE\n3\n0.5308 10 5 12500\n0.5308 20 5 12500\n0.5308 30 5 12500")
+        text = text.replace("TIME\n0 2000 0.5 0.5", "TIME\n0 40 0.5 0.5")
+        d = tempfile.mkdtemp()
+        path = os.path.join(d, "c1_small.key")
+        with open(path, "w") as f:
+            f.write(text)
+        prob = heom.Problem.from_key(path)
+        prob.prepare_sample()
+        plan = heom.Plan(prob, precision[3:])
+        t0 = time.perf_counter()
+        P, _ = plan.run_2des()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        shutil.rmtree(d, ignore_errors=True)
+        print(f"profile run: FMO 2DES point, {len(P)} P values, {wall * 1e3:.1f} ms wall, {plan.describe()}")
+        return
     prob = heom.Problem.from_key(KEY)
     prob.prepare_sample()
     rows = [(a, b, c, c + 50.0) for a, b, c, _ in scan_rows()[:148]]
@@ -386,7 +412,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--profile-run", default=None, choices=["fp32-bulk", "fp64"],
+    ap.add_argument("--profile-run", default=None, choices=["fp32-bulk", "fp64", "c1-fp32-bulk", "c1-fp64", "c1-fp64-exact"],
                     help="run only a small scan of that precision (for profiler captures)")
     a = ap.parse_args()
     if a.profile_run:

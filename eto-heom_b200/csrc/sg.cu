@@ -390,7 +390,7 @@ int sg_run(SgState &s, const heom::Problem &p, int C, const int mask[3], const h
     if (e != cudaSuccess) return fail(HEOM_ERR_NOMEM, "staged path state: out of device memory");
     s.state_bytes = state_bytes;
   }
-  if (total > s.P_cap) {
+  if (total > s.P_cap || !s.d_P) { // allocated even when nothing is recorded
     if (s.d_P) cudaFree(s.d_P);
     s.d_P = nullptr;
     s.P_cap = 0;
@@ -460,7 +460,7 @@ int sg_run(SgState &s, const heom::Problem &p, int C, const int mask[3], const h
   const int reps = (S_max + s.g_chunk - 1) / s.g_chunk;
   for (int r = 0; r < reps; r++) SGCK(cudaGraphLaunch(s.gexec, st));
   s.launches += (long long)reps * (4LL * s.g_chunk + 1);
-  SGCK(cudaMemcpyAsync(P, s.d_P, sizeof(double2) * total, cudaMemcpyDeviceToHost, st));
+  if (total > 0) SGCK(cudaMemcpyAsync(P, s.d_P, sizeof(double2) * total, cudaMemcpyDeviceToHost, st));
   SGCK(cudaStreamSynchronize(st));
   for (long long q = 0; q < 2 * total; q++)
     if (!std::isfinite(P[q])) return fail(HEOM_ERR_NUMERIC, "non-finite P(t): the propagation diverged");

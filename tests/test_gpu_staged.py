@@ -82,3 +82,19 @@ def test_c3_chain_precision_study():
     print(f"c3 chain (N=13, 2925 ADOs, 6001 steps): fp64 staged vs exact {e64:.2e}; "
           f"fp32-bulk vs fp64 {e32:.2e}; fp32-bulk vs exact {e32x:.2e}")
     assert e64 <= 1e-10 and e32x <= 1e-5
+
+
+@pytest.mark.parametrize("precision", ["fp64-exact", "fp64", "fp32-bulk"])
+def test_run_with_no_records(tmp_path, precision):
+    """A key whose end time precedes pulse 3 records nothing (the reference prints no line)."""
+    heom = load_pkg()
+    with open(key("c4_trimer_short.key")) as f:
+        text = f.read()
+    assert "TIME\n0 160 0.5 0.5" in text
+    k = tmp_path / "early_end.key"
+    k.write_text(text.replace("TIME\n0 160 0.5 0.5", "TIME\n0 40 0.5 0.5"))
+    prob = heom.Problem.from_key(str(k))
+    prob.prepare_sample()
+    assert prob.info.n_record == 0
+    P, tr = heom.Plan(prob, precision).run_2des()
+    assert len(P) == 0 and all(len(t) == 0 for t in tr)
