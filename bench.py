@@ -391,7 +391,7 @@ def profile_run(precision: str):
         prob.prepare_sample()
         plan = heom.Plan(prob, precision[3:])
         t0 = time.perf_counter()
-        P, _ = plan.run_2des()
+        P, _ = plan.run_2des(trajectories=False)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         shutil.rmtree(d, ignore_errors=True)

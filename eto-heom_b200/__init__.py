@@ -271,13 +271,16 @@ class Plan:
                                           _dptr(out), cap, ctypes.byref(n)))
         return out[:, :n.value]
 
-    def run_2des(self):
+    def run_2des(self, trajectories: bool = True):
+        """CPU_2DES's combined p111 - p110 - p101 and, unless trajectories=False, the
+        three mask trajectories (None otherwise; the staged path then propagates the
+        combined point only)."""
         cap = max(self.problem.info.n_record, 1)
         P = np.zeros(cap, dtype=np.complex128)
-        tr = np.zeros((3, cap), dtype=np.complex128)
+        tr = np.zeros((3, cap), dtype=np.complex128) if trajectories else None
         n = ctypes.c_int()
-        _check(lib().heom_run_2des(self._h, _dptr(P), _dptr(tr), cap, ctypes.byref(n)))
-        return P[:n.value], tr[:, :n.value]
+        _check(lib().heom_run_2des(self._h, _dptr(P), _dptr(tr) if trajectories else None, cap, ctypes.byref(n)))
+        return P[:n.value], (tr[:, :n.value] if trajectories else None)
 
     def scan_layout(self, points: np.ndarray):
         pts = np.ascontiguousarray(points, dtype=SCAN_POINT_DTYPE)

@@ -73,19 +73,58 @@ struct SgTab {
 
 const char *sg_last_error() { return sg_err.c_str(); }
 
+// Shared-memory geometry of sg_stage.  Blocks are stored with rows padded to Np (a
+// multiple of 4) plus 2, so that a thread's 4-wide column strip is one or two 16-byte
+// loads and the rows of a warp's tile fall in different banks.
+__host__ __device__ inline int sg_np(int N) { return (N + 3) & ~3; }
+__host__ __device__ inline int sg_stride(int N) { return sg_np(N) + 2; }
+// Strip slots per ADO: N rows x Np/4 strips, laid out linearly for Np <= 16 and in warp
+// tiles of 8 rows x 4 strips (conflict-free strip loads) for wider blocks.
+__host__ __device__ inline int sg_slots_per_ado(int N) {
+  const int spr = sg_np(N) / 4;
+  return spr <= 4 ? N * spr : ((N + 7) / 8) * ((spr + 3) / 4) * 32;
+}
+// T2 elements of dynamic shared memory: own operator, P2, P3 (N x S each), the own and
+// up to two source blocks of apc ADOs (N x S each), the commutator of apc ADOs (N x N).
+__host__ __device__ inline size_t sg_smem_elems(int N, int apc) {
+  return (size_t)(3 + 3 * apc) * N * sg_stride(N) + (size_t)apc * N * N;
+}
+
+template <typename T> struct Quad;
+template <> struct Quad<float> {
+  static __device__ __forceinline__ void load(const float2 *p, float2 (&v)[4]) {
+    const float4 u = *reinterpret_cast<const float4 *>(p), w = *reinterpret_cast<const float4 *>(p + 2);
+    v[0] = make_float2(u.x, u.y);
+    v[1] = make_float2(u.z, u.w);
+    v[2] = make_float2(w.x, w.y);
+    v[3] = make_float2(w.z, w.w);
+  }
+};
+template <> struct Quad<double> {
+  static __device__ __forceinline__ void load(const double2 *p, double2 (&v)[4]) {
+    for (int e = 0; e < 4; e++) v[e] = p[e];
+  }
+};
+
+// One Horner stage over (ADO tile, component, point).  Phase 1: each thread forms the
+// commutator -- own operator plus sources -- of a 1 x 4 strip (r, c0..c0+3) of one ADO
+// block from shared memory, with the per-element operation order of a plain
+// element-per-thread loop.  Phase 2: element-per-thread (coalesced) bath couplings,
+// FP64 diagonal and damping, and the Horner update.
 template <typename T>
-__global__ void __launch_bounds__(1024) sg_stage(SgArgs a, int m, int step_local, const int *__restrict__ base) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) sg_stage(SgArgs a, int m, int step_local, const int *__restrict__ base) {
   using T2 = typename Vec2<T>::t;
   const int p = blockIdx.z, cq = blockIdx.y;
   const int i = *base + step_local;
   if (i >= a.nsteps[p]) return;
   const int N = a.N, NN = N * N, nado = a.n_ado, M = a.M, K = a.K, Km = a.Km;
+  const int S = sg_stride(N), NS = N * S, spr = sg_np(N) / 4;
   const int tid = threadIdx.x, bs = blockDim.x;
   const int apc = a.apc;
   extern __shared__ __align__(16) unsigned char smraw[];
-  T2 *A = (T2 *)smraw;             // A[q] (q = 0..3), S2, S3
-  T2 *wb = A + 6 * NN;             // own blocks
-  __shared__ double2 s_tr[2];
+  T2 *Am = (T2 *)smraw;         // [3][N][S]: own operator, P2, P3
+  T2 *Wm = Am + 3 * NS;         // [3][apc][N][S]: own blocks, first and second source blocks
+  T2 *Xm = Wm + 3 * apc * NS;   // [apc][N][N]: commutator
   const int g = 4 * i + (4 - m);   // global stage index: buffers alternate every stage
   const double2 *w64_in = (g & 1) ? a.w64b : a.w64a;
   double2 *w64_out = (g & 1) ? a.w64a : a.w64b;
@@ -101,26 +140,54 @@ __global__ void __launch_bounds__(1024) sg_stage(SgArgs a, int m, int step_local
     if (a.C == 1) on[q] = on[q] && a.mask[q];
     ef[q] = a.field[si * 3 + q];
   }
-  for (int t = tid; t < NN; t += bs) {
-    double vr[3], vi[3];
-    for (int q = 0; q < 3; q++) {
-      const double2 x = a.Xs[q * NN + t];
-      vr[q] = on[q] ? -(x.x * ef[q].x - x.y * ef[q].y) : 0.0;
-      vi[q] = on[q] ? -(x.x * ef[q].y + x.y * ef[q].x) : 0.0;
+  // mixed-difference sources of this component: D2 <- P2 R, D3 <- P3 R, Q <- P2 D3 + P3 D2
+  // (operator index in Am, source component) of source 1 and source 2
+  int nsrc = 0, op1 = 0, from1 = 0, op2 = 0, from2 = 0;
+  if (a.C == 4) {
+    if (cq == 1 && on[1]) { op1 = 1; from1 = 0; nsrc = 1; }
+    if (cq == 2 && on[2]) { op1 = 2; from1 = 0; nsrc = 1; }
+    if (cq == 3) {
+      if (on[1]) { op1 = 1; from1 = 2; nsrc = 1; }
+      if (on[2]) {
+        if (nsrc == 0) { op1 = 2; from1 = 1; }
+        else { op2 = 2; from2 = 1; }
+        nsrc++;
+      }
     }
-    const double br = a.Hoff[t].x + vr[0], bi = a.Hoff[t].y + vi[0];
-    A[t] = to2<T>(br, bi);
-    A[NN + t] = to2<T>(br + vr[1], bi + vi[1]);
-    A[2 * NN + t] = to2<T>(br + vr[2], bi + vi[2]);
-    A[3 * NN + t] = to2<T>(br + vr[1] + vr[2], bi + vi[1] + vi[2]);
-    A[4 * NN + t] = to2<T>(vr[1], vi[1]);
-    A[5 * NN + t] = to2<T>(vr[2], vi[2]);
-    if (a.C == 1) A[t] = to2<T>(br + vr[1] + vr[2], bi + vi[1] + vi[2]);
+  }
+  const T2 zero = to2<T>(0.0, 0.0);
+  for (int t = tid; t < NS; t += bs) {
+    const int r = t / S, c = t - r * S;
+    T2 own = zero, p2 = zero, p3 = zero;
+    if (c < N) {
+      const int e = r * N + c;
+      double vr[3], vi[3];
+      for (int q = 0; q < 3; q++) {
+        const double2 x = a.Xs[q * NN + e];
+        vr[q] = on[q] ? -(x.x * ef[q].x - x.y * ef[q].y) : 0.0;
+        vi[q] = on[q] ? -(x.x * ef[q].y + x.y * ef[q].x) : 0.0;
+      }
+      const double br = a.Hoff[e].x + vr[0], bi = a.Hoff[e].y + vi[0];
+      if (a.C == 1 || cq == 3) own = to2<T>(br + vr[1] + vr[2], bi + vi[1] + vi[2]);
+      else if (cq == 1) own = to2<T>(br + vr[1], bi + vi[1]);
+      else if (cq == 2) own = to2<T>(br + vr[2], bi + vi[2]);
+      else own = to2<T>(br, bi);
+      p2 = to2<T>(vr[1], vi[1]);
+      p3 = to2<T>(vr[2], vi[2]);
+    }
+    Am[t] = own;
+    Am[NS + t] = p2;
+    Am[2 * NS + t] = p3;
   }
   const int n0 = blockIdx.x * apc;
-  for (int t = tid; t < apc * NN; t += bs) {
-    const int n = n0 + t / NN;
-    if (n < nado) wb[t] = w32_in[pb + (size_t)(cq * nado + n) * NN + (t % NN)];
+  for (int b = 0; b <= nsrc; b++) {
+    const int comp = b == 0 ? cq : b == 1 ? from1 : from2;
+    T2 *Wb = Wm + (size_t)b * apc * NS;
+    for (int t = tid; t < apc * NS; t += bs) {
+      const int nl = t / NS, rc = t - nl * NS, r = rc / S, c = rc - r * S;
+      const int n = n0 + nl;
+      Wb[t] = (n < nado && c < N) ? w32_in[pb + (size_t)(comp * nado + n) * NN + r * N + c] : zero;
+    }
   }
   __syncthreads();
   // P before the step, from the FP64 state of ADO 0 (first stage of the step only)
@@ -146,50 +213,63 @@ __global__ void __launch_bounds__(1024) sg_stage(SgArgs a, int m, int step_local
       if (tid == 0) a.P[a.offsets[p] + rec] = make_double2(sr, sim);
     }
   }
-  const bool src = a.C == 4 && (on[1] || on[2]) && cq > 0;
-  const T2 *Ac = A + (a.C == 4 ? cq : 0) * NN;
+  // phase 1: X = sum over (operator O, block Z) of O Z - Z O, one 1 x 4 strip per slot
+  const int per_ado = sg_slots_per_ado(N);
+  const int cg = (spr + 3) / 4;
+  for (int s = tid; s < apc * per_ado; s += bs) {
+    const int nl = s / per_ado, u = s - nl * per_ado;
+    int r, cs;
+    if (spr <= 4) {
+      r = u / spr;
+      cs = u - r * spr;
+    } else {
+      const int tile = u >> 5, lane = u & 31;
+      r = (tile / cg) * 8 + (lane >> 2);
+      cs = (tile % cg) * 4 + (lane & 3);
+      if (r >= N || cs >= spr) continue;
+    }
+    const int c0 = 4 * cs;
+    T xr[4] = {0, 0, 0, 0}, xi[4] = {0, 0, 0, 0};
+    for (int b = 0; b <= nsrc; b++) {
+      const T2 *Ab = Am + (b == 0 ? 0 : b == 1 ? op1 : op2) * NS;
+      const T2 *Wb = Wm + ((size_t)b * apc + nl) * NS;
+      for (int l = 0; l < N; l++) {
+        const T2 a1 = Ab[r * S + l], z2 = Wb[r * S + l];
+        T2 z1[4], a2[4];
+        Quad<T>::load(Wb + l * S + c0, z1);
+        Quad<T>::load(Ab + l * S + c0, a2);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          xr[e] = fma(a1.x, z1[e].x, xr[e]);
+          xr[e] = fma(-a1.y, z1[e].y, xr[e]);
+          xi[e] = fma(a1.x, z1[e].y, xi[e]);
+          xi[e] = fma(a1.y, z1[e].x, xi[e]);
+          xr[e] = fma(-z2.x, a2[e].x, xr[e]);
+          xr[e] = fma(z2.y, a2[e].y, xr[e]);
+          xi[e] = fma(-z2.x, a2[e].y, xi[e]);
+          xi[e] = fma(-z2.y, a2[e].x, xi[e]);
+        }
+      }
+    }
+    T2 *Xr = Xm + (size_t)nl * NN + r * N;
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      if (c0 + e < N) {
+        T2 v;
+        v.x = xr[e];
+        v.y = xi[e];
+        Xr[c0 + e] = v;
+      }
+  }
+  __syncthreads();
+  // phase 2: k = -i X + bath couplings + FP64 diagonal/damping; Horner update
   const double cm = a.h / m;
   for (int t = tid; t < apc * NN; t += bs) {
     const int nl = t / NN, n = n0 + nl;
     if (n >= nado) continue;
     const int rc = t - nl * NN, r = rc / N, c = rc - r * N;
-    const T2 *wl = wb + nl * NN;
-    T xr = 0, xi = 0; // X = A w - w A
-    for (int l = 0; l < N; l++) {
-      const T2 a1 = Ac[r * N + l], z1 = wl[l * N + c], z2 = wl[r * N + l], a2 = Ac[l * N + c];
-      xr = fma(a1.x, z1.x, xr);
-      xr = fma(-a1.y, z1.y, xr);
-      xi = fma(a1.x, z1.y, xi);
-      xi = fma(a1.y, z1.x, xi);
-      xr = fma(-z2.x, a2.x, xr);
-      xr = fma(z2.y, a2.y, xr);
-      xi = fma(-z2.x, a2.y, xi);
-      xi = fma(-z2.y, a2.x, xi);
-    }
-    if (src) {
-      for (int s2 = 0; s2 < 2; s2++) {
-        int from = -1, op = 0;
-        if (cq == 1 && s2 == 0 && on[1]) { from = 0; op = 4; }
-        if (cq == 2 && s2 == 0 && on[2]) { from = 0; op = 5; }
-        if (cq == 3 && s2 == 0 && on[1]) { from = 2; op = 4; }
-        if (cq == 3 && s2 == 1 && on[2]) { from = 1; op = 5; }
-        if (from < 0) continue;
-        const T2 *Sm = A + op * NN;
-        const T2 *wf = w32_in + pb + (size_t)(from * nado + n) * NN;
-        for (int l = 0; l < N; l++) {
-          const T2 a1 = Sm[r * N + l], z1 = wf[l * N + c], z2 = wf[r * N + l], a2 = Sm[l * N + c];
-          xr = fma(a1.x, z1.x, xr);
-          xr = fma(-a1.y, z1.y, xr);
-          xi = fma(a1.x, z1.y, xi);
-          xi = fma(a1.y, z1.x, xi);
-          xr = fma(-z2.x, a2.x, xr);
-          xr = fma(z2.y, a2.y, xr);
-          xi = fma(-z2.x, a2.y, xi);
-          xi = fma(-z2.y, a2.x, xi);
-        }
-      }
-    }
-    T kr = xi, ki = -xr; // -i X
+    const T2 x = Xm[t];
+    T kr = x.y, ki = -x.x; // -i X
     for (int pass = 0; pass < 2; pass++) {
       const int s = pass == 0 ? r : c;
       if (s < 1 || s > K || (pass == 1 && c == r)) continue;
@@ -198,10 +278,10 @@ __global__ void __launch_bounds__(1024) sg_stage(SgArgs a, int m, int step_local
         const int o = n * M + j + k * K;
         const int u = a.up[o], d = a.dn[o];
         if (u >= 0 && dr != dc) {
-          const T x = (T)a.xc[o] * (T)(dc - dr);
+          const T xx = (T)a.xc[o] * (T)(dc - dr);
           const T2 z = w32_in[pb + (size_t)(cq * nado + u) * NN + rc];
-          kr = fma(x, z.y, kr);
-          ki = fma(-x, z.x, ki);
+          kr = fma(xx, z.y, kr);
+          ki = fma(-xx, z.x, ki);
         }
         if (d >= 0) {
           const T y = (T)a.yc[o];
@@ -268,11 +348,12 @@ int sg_init(SgState &s, const heom::Problem &p, int precision, cudaStream_t st) 
   s.stride = p.print_stride();
   s.h = (double)p.step_size;
   const int NN = s.N * s.N;
-  s.apc = std::max(1, 256 / NN);
-  s.threads = std::min(1024, ((s.apc * NN + 31) / 32) * 32);
-  if (s.apc * NN > 1024) s.apc = 1;
+  // about 256 strip slots per CTA (one ADO for N > 16), at most 256 threads
+  const int slots = sg_slots_per_ado(s.N);
+  s.apc = std::max(1, 256 / slots);
+  s.threads = std::min(256, ((s.apc * slots + 31) / 32) * 32);
   const size_t tsz = s.precision == HEOM_FP64 ? 16 : 8;
-  s.smem = tsz * (6 * NN + (size_t)s.apc * NN);
+  s.smem = tsz * sg_smem_elems(s.N, s.apc);
   int max_smem = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
