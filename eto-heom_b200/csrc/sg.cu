@@ -48,6 +48,8 @@ struct SgArgs {
   double2 *rho, *w64a, *w64b;
   void *w32a, *w32b;
   double2 *P;
+  unsigned char *ops;    // per (point, component): the step's operators and their ranges
+  long long ops_stride;  // bytes per (point, component)
 };
 
 // Table layout in one allocation (byte offsets, 256-aligned sections).
@@ -90,6 +92,13 @@ __host__ __device__ inline size_t sg_smem_elems(int N, int apc) {
   return (size_t)(3 + 3 * apc) * N * sg_stride(N) + (size_t)apc * N * N;
 }
 
+constexpr int kSgMaxN = 32;
+// Bytes of one (point, component) entry of the operator buffer: own operator, P2, P3
+// (N x S each, T2) and int ranges [3][4][kSgMaxN] (row lo/hi, column lo/hi).
+__host__ __device__ inline size_t sg_ops_bytes(int N, size_t tsz) {
+  return ((3 * (size_t)N * sg_stride(N) * tsz + 3 * 4 * kSgMaxN * sizeof(int)) + 255) & ~(size_t)255;
+}
+
 template <typename T> struct Quad;
 template <> struct Quad<float> {
   static __device__ __forceinline__ void load(const float2 *p, float2 (&v)[4]) {
@@ -106,11 +115,83 @@ template <> struct Quad<double> {
   }
 };
 
+// The operators of one step, once per (component, point): own operator A_q (off-diagonal
+// H plus the pulses on for component q), P2 and P3 (the source operators), padded to
+// rows of S, and for each the range [lo, hi) of nonzero entries of every row and
+// column (lo = 32767, hi = 0 when empty).  Rows and columns outside the ranges hold
+// exact zeros, so the stage kernel's commutator loops skip them without changing any
+// partial sum.
+template <typename T>
+__global__ void __launch_bounds__(256) sg_ops(SgArgs a, int step_local, const int *__restrict__ base) {
+  using T2 = typename Vec2<T>::t;
+  const int cq = blockIdx.x, p = blockIdx.y;
+  const int i = *base + step_local;
+  if (i >= a.nsteps[p]) return;
+  const int N = a.N, NN = N * N, S = sg_stride(N), NS = N * S;
+  const int tid = threadIdx.x, bs = blockDim.x;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T2 *Om = (T2 *)smraw;
+  unsigned char *gb = a.ops + (size_t)(p * a.C + cq) * a.ops_stride;
+  T2 *Og = (T2 *)gb;
+  int *Rg = (int *)(gb + 3 * (size_t)NS * sizeof(T2));
+  const size_t si = (size_t)p * a.S_max + i;
+  const unsigned f = a.flags[si];
+  int on[3];
+  double2 ef[3];
+  for (int q = 0; q < 3; q++) {
+    on[q] = (f >> q) & 1;
+    if (a.C == 1) on[q] = on[q] && a.mask[q];
+    ef[q] = a.field[si * 3 + q];
+  }
+  const T2 zero = to2<T>(0.0, 0.0);
+  for (int t = tid; t < NS; t += bs) {
+    const int r = t / S, c = t - r * S;
+    T2 own = zero, p2 = zero, p3 = zero;
+    if (c < N) {
+      const int e = r * N + c;
+      double vr[3], vi[3];
+      for (int q = 0; q < 3; q++) {
+        const double2 x = a.Xs[q * NN + e];
+        vr[q] = on[q] ? -(x.x * ef[q].x - x.y * ef[q].y) : 0.0;
+        vi[q] = on[q] ? -(x.x * ef[q].y + x.y * ef[q].x) : 0.0;
+      }
+      const double br = a.Hoff[e].x + vr[0], bi = a.Hoff[e].y + vi[0];
+      if (a.C == 1 || cq == 3) own = to2<T>(br + vr[1] + vr[2], bi + vi[1] + vi[2]);
+      else if (cq == 1) own = to2<T>(br + vr[1], bi + vi[1]);
+      else if (cq == 2) own = to2<T>(br + vr[2], bi + vi[2]);
+      else own = to2<T>(br, bi);
+      p2 = to2<T>(vr[1], vi[1]);
+      p3 = to2<T>(vr[2], vi[2]);
+    }
+    Om[t] = own;
+    Om[NS + t] = p2;
+    Om[2 * NS + t] = p3;
+    Og[t] = own;
+    Og[NS + t] = p2;
+    Og[2 * NS + t] = p3;
+  }
+  __syncthreads();
+  for (int t = tid; t < 3 * 2 * kSgMaxN; t += bs) {
+    const int o = t / (2 * kSgMaxN), kind = (t / kSgMaxN) & 1, j = t % kSgMaxN;
+    int lo = 32767, hi = 0;
+    if (j < N)
+      for (int l = 0; l < N; l++) {
+        const T2 v = kind == 0 ? Om[o * NS + j * S + l] : Om[o * NS + l * S + j];
+        if (v.x != (T)0 || v.y != (T)0) {
+          lo = min(lo, l);
+          hi = l + 1;
+        }
+      }
+    Rg[(o * 4 + 2 * kind) * kSgMaxN + j] = lo;
+    Rg[(o * 4 + 2 * kind + 1) * kSgMaxN + j] = hi;
+  }
+}
+
 // One Horner stage over (ADO tile, component, point).  Phase 1: each thread forms the
-// commutator -- own operator plus sources -- of a 1 x 4 strip (r, c0..c0+3) of one ADO
-// block from shared memory, with the per-element operation order of a plain
-// element-per-thread loop.  Phase 2: element-per-thread (coalesced) bath couplings,
-// FP64 diagonal and damping, and the Horner update.
+// commutator -- own operator plus sources, operators from sg_ops -- of a 1 x 4 strip
+// (r, c0..c0+3) of one ADO block from shared memory, over the nonzero rows/columns of
+// each operator only.  Phase 2: element-per-thread (coalesced) bath couplings, FP64
+// diagonal and damping, and the Horner update.
 template <typename T>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) sg_stage(SgArgs a, int m, int step_local, const int *__restrict__ base) {
   using T2 = typename Vec2<T>::t;
@@ -134,12 +215,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) sg_stage(SgArgs a
   const size_t si = (size_t)p * a.S_max + i;
   const unsigned f = a.flags[si];
   int on[3];
-  double2 ef[3];
-  for (int q = 0; q < 3; q++) {
-    on[q] = (f >> q) & 1;
-    if (a.C == 1) on[q] = on[q] && a.mask[q];
-    ef[q] = a.field[si * 3 + q];
-  }
+  for (int q = 0; q < 3; q++) on[q] = (f >> q) & 1;
   // mixed-difference sources of this component: D2 <- P2 R, D3 <- P3 R, Q <- P2 D3 + P3 D2
   // (operator index in Am, source component) of source 1 and source 2
   int nsrc = 0, op1 = 0, from1 = 0, op2 = 0, from2 = 0;
@@ -156,28 +232,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) sg_stage(SgArgs a
     }
   }
   const T2 zero = to2<T>(0.0, 0.0);
-  for (int t = tid; t < NS; t += bs) {
-    const int r = t / S, c = t - r * S;
-    T2 own = zero, p2 = zero, p3 = zero;
-    if (c < N) {
-      const int e = r * N + c;
-      double vr[3], vi[3];
-      for (int q = 0; q < 3; q++) {
-        const double2 x = a.Xs[q * NN + e];
-        vr[q] = on[q] ? -(x.x * ef[q].x - x.y * ef[q].y) : 0.0;
-        vi[q] = on[q] ? -(x.x * ef[q].y + x.y * ef[q].x) : 0.0;
-      }
-      const double br = a.Hoff[e].x + vr[0], bi = a.Hoff[e].y + vi[0];
-      if (a.C == 1 || cq == 3) own = to2<T>(br + vr[1] + vr[2], bi + vi[1] + vi[2]);
-      else if (cq == 1) own = to2<T>(br + vr[1], bi + vi[1]);
-      else if (cq == 2) own = to2<T>(br + vr[2], bi + vi[2]);
-      else own = to2<T>(br, bi);
-      p2 = to2<T>(vr[1], vi[1]);
-      p3 = to2<T>(vr[2], vi[2]);
+  __shared__ int s_rng[3 * 4 * kSgMaxN];
+  {
+    const unsigned char *gb = a.ops + (size_t)(p * a.C + cq) * a.ops_stride;
+    const int *Rg = (const int *)(gb + 3 * (size_t)NS * sizeof(T2));
+    for (int t = tid; t < 3 * 4 * kSgMaxN; t += bs) s_rng[t] = Rg[t];
+    const int nv = NS * (int)sizeof(T2) / 16; // 16-byte vectors per operator
+    for (int b = 0; b <= nsrc; b++) {
+      const int o = b == 0 ? 0 : b == 1 ? op1 : op2;
+      const uint4 *src = (const uint4 *)(gb + (size_t)o * NS * sizeof(T2));
+      uint4 *dst = (uint4 *)(Am + (size_t)o * NS);
+      for (int t = tid; t < nv; t += bs) dst[t] = src[t];
     }
-    Am[t] = own;
-    Am[NS + t] = p2;
-    Am[2 * NS + t] = p3;
   }
   const int n0 = blockIdx.x * apc;
   for (int b = 0; b <= nsrc; b++) {
@@ -231,19 +297,36 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) sg_stage(SgArgs a
     const int c0 = 4 * cs;
     T xr[4] = {0, 0, 0, 0}, xi[4] = {0, 0, 0, 0};
     for (int b = 0; b <= nsrc; b++) {
-      const T2 *Ab = Am + (b == 0 ? 0 : b == 1 ? op1 : op2) * NS;
+      const int o = b == 0 ? 0 : b == 1 ? op1 : op2;
+      const T2 *Ab = Am + o * NS;
       const T2 *Wb = Wm + ((size_t)b * apc + nl) * NS;
-      for (int l = 0; l < N; l++) {
-        const T2 a1 = Ab[r * S + l], z2 = Wb[r * S + l];
-        T2 z1[4], a2[4];
+      const int *rg = s_rng + o * 4 * kSgMaxN;
+      // A W: the nonzero entries of row r of A
+      for (int l = rg[r], le = rg[kSgMaxN + r]; l < le; l++) {
+        const T2 a1 = Ab[r * S + l];
+        T2 z1[4];
         Quad<T>::load(Wb + l * S + c0, z1);
-        Quad<T>::load(Ab + l * S + c0, a2);
 #pragma unroll
         for (int e = 0; e < 4; e++) {
           xr[e] = fma(a1.x, z1[e].x, xr[e]);
           xr[e] = fma(-a1.y, z1[e].y, xr[e]);
           xi[e] = fma(a1.x, z1[e].y, xi[e]);
           xi[e] = fma(a1.y, z1[e].x, xi[e]);
+        }
+      }
+      // - W A: the nonzero entries of columns c0..c0+3 of A
+      int lo = rg[2 * kSgMaxN + c0], hi = rg[3 * kSgMaxN + c0];
+#pragma unroll
+      for (int e = 1; e < 4; e++) {
+        lo = min(lo, rg[2 * kSgMaxN + c0 + e]);
+        hi = max(hi, rg[3 * kSgMaxN + c0 + e]);
+      }
+      for (int l = lo; l < hi; l++) {
+        const T2 z2 = Wb[r * S + l];
+        T2 a2[4];
+        Quad<T>::load(Ab + l * S + c0, a2);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
           xr[e] = fma(-z2.x, a2[e].x, xr[e]);
           xr[e] = fma(z2.y, a2[e].y, xr[e]);
           xi[e] = fma(-z2.x, a2[e].y, xi[e]);
@@ -360,6 +443,9 @@ int sg_init(SgState &s, const heom::Problem &p, int precision, cudaStream_t st) 
   if (NN > 1024 || s.smem > (size_t)max_smem) return fail(HEOM_ERR_UNSUPPORTED, "system too large for the staged path");
   SGCK(cudaFuncSetAttribute(sg_stage<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem));
   SGCK(cudaFuncSetAttribute(sg_stage<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem));
+  const int ops_smem = (int)(3 * (size_t)s.N * sg_stride(s.N) * tsz);
+  SGCK(cudaFuncSetAttribute(sg_ops<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, ops_smem));
+  SGCK(cudaFuncSetAttribute(sg_ops<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ops_smem));
   SgTab tl(s.N, s.n_ado, s.M, s.K_m);
   s.tab_bytes = tl.total;
   SGCK(cudaMalloc(&s.d_tab, tl.total));
@@ -462,7 +548,11 @@ int sg_run(SgState &s, const heom::Problem &p, int C, const int mask[3], const h
   const int E_pt = C * s.n_ado * NN;
   const long long E = (long long)n * E_pt;
   const bool d = s.precision == HEOM_FP64;
-  const size_t state_bytes = a256(16 * E) * 3 + (d ? 0 : a256(8 * E) * 2);
+  // rho and the FP64 iterate w64 (16 B each), plus: FP64 path -- a second w64 buffer,
+  // read by neighbours while the other is written; FP32-bulk -- two FP32 copies for the
+  // neighbours and shared blocks, w64 then being read and written only by its own
+  // element's thread, in place.
+  const size_t state_bytes = a256(16 * E) * (d ? 3 : 2) + (d ? 0 : a256(8 * E) * 2);
   if (state_bytes > s.state_bytes) {
     if (s.d_state) cudaFree(s.d_state);
     s.d_state = nullptr;
@@ -470,6 +560,15 @@ int sg_run(SgState &s, const heom::Problem &p, int C, const int mask[3], const h
     cudaError_t e = cudaMalloc(&s.d_state, state_bytes);
     if (e != cudaSuccess) return fail(HEOM_ERR_NOMEM, "staged path state: out of device memory");
     s.state_bytes = state_bytes;
+  }
+  const size_t ops_stride = sg_ops_bytes(s.N, d ? 16 : 8);
+  const size_t ops_bytes = ops_stride * (size_t)n * C;
+  if (ops_bytes > s.ops_bytes) {
+    if (s.d_ops) cudaFree(s.d_ops);
+    s.d_ops = nullptr;
+    s.ops_bytes = 0;
+    SGCK(cudaMalloc(&s.d_ops, ops_bytes));
+    s.ops_bytes = ops_bytes;
   }
   if (total > s.P_cap || !s.d_P) { // allocated even when nothing is recorded
     if (s.d_P) cudaFree(s.d_P);
@@ -509,10 +608,12 @@ int sg_run(SgState &s, const heom::Problem &p, int C, const int mask[3], const h
   a.offsets = (const long long *)(sb + off_off);
   a.rho = (double2 *)stb;
   a.w64a = (double2 *)(stb + a256(16 * E));
-  a.w64b = (double2 *)(stb + 2 * a256(16 * E));
-  a.w32a = d ? (void *)a.w64a : (void *)(stb + 3 * a256(16 * E));
-  a.w32b = d ? (void *)a.w64b : (void *)(stb + 3 * a256(16 * E) + a256(8 * E));
+  a.w64b = d ? (double2 *)(stb + 2 * a256(16 * E)) : a.w64a;
+  a.w32a = d ? (void *)a.w64a : (void *)(stb + 2 * a256(16 * E));
+  a.w32b = d ? (void *)a.w64b : (void *)(stb + 2 * a256(16 * E) + a256(8 * E));
   a.P = s.d_P;
+  a.ops = (unsigned char *)s.d_ops;
+  a.ops_stride = (long long)ops_stride;
   SGCK(cudaMemsetAsync(s.d_P, 0, sizeof(double2) * std::max<long long>(total, 1), st));
   if (d) sg_init_state<double><<<1024, 256, 0, st>>>(a, E);
   else sg_init_state<float><<<1024, 256, 0, st>>>(a, E);
@@ -525,11 +626,16 @@ int sg_run(SgState &s, const heom::Problem &p, int C, const int mask[3], const h
   cudaGraph_t graph;
   SGCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   dim3 grid((s.n_ado + s.apc - 1) / s.apc, C, n);
-  for (int k = 0; k < s.g_chunk; k++)
+  const dim3 ogrid(C, n);
+  const size_t osmem = 3 * (size_t)s.N * sg_stride(s.N) * (d ? 16 : 8);
+  for (int k = 0; k < s.g_chunk; k++) {
+    if (d) sg_ops<double><<<ogrid, 256, osmem, st>>>(a, k, s.d_base);
+    else sg_ops<float><<<ogrid, 256, osmem, st>>>(a, k, s.d_base);
     for (int m = 4; m >= 1; m--) {
       if (d) sg_stage<double><<<grid, s.threads, s.smem, st>>>(a, m, k, s.d_base);
       else sg_stage<float><<<grid, s.threads, s.smem, st>>>(a, m, k, s.d_base);
     }
+  }
   sg_bump<<<1, 1, 0, st>>>(s.d_base, s.g_chunk);
   cudaError_t le = cudaGetLastError();
   cudaError_t ce = cudaStreamEndCapture(st, &graph);
@@ -540,7 +646,7 @@ int sg_run(SgState &s, const heom::Problem &p, int C, const int mask[3], const h
   if (ie != cudaSuccess) return fail(HEOM_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ie));
   const int reps = (S_max + s.g_chunk - 1) / s.g_chunk;
   for (int r = 0; r < reps; r++) SGCK(cudaGraphLaunch(s.gexec, st));
-  s.launches += (long long)reps * (4LL * s.g_chunk + 1);
+  s.launches += (long long)reps * (5LL * s.g_chunk + 1);
   if (total > 0) SGCK(cudaMemcpyAsync(P, s.d_P, sizeof(double2) * total, cudaMemcpyDeviceToHost, st));
   SGCK(cudaStreamSynchronize(st));
   for (long long q = 0; q < 2 * total; q++)
@@ -554,6 +660,7 @@ void sg_release(SgState &s) {
   if (s.d_state) cudaFree(s.d_state);
   if (s.d_sched) cudaFree(s.d_sched);
   if (s.d_P) cudaFree(s.d_P);
+  if (s.d_ops) cudaFree(s.d_ops);
   if (s.d_base) cudaFree(s.d_base);
   s = SgState();
 }

@@ -32,6 +32,8 @@ struct SgState {
   size_t sched_bytes = 0;
   double2 *d_P = nullptr;
   long long P_cap = 0;
+  void *d_ops = nullptr;              // per (point, component): the step's operators
+  size_t ops_bytes = 0;
   int *d_base = nullptr;
   // graph of one chunk of steps of the current run
   cudaGraphExec_t gexec = nullptr;
