@@ -198,6 +198,59 @@ def run_reference_arm(a):
 
 
 # ------------------------------------------------------------------ our arm
+C1_KEY = os.path.join(ROOT, "tests", "golden", "keys", "c1_fmo.key")
+
+
+def large_n_record(heom, device: int, fp32_peak: float) -> dict:
+    """The FMO aggregate (N = 29 with the two-exciton manifold, K = 14, L = 3, 680 ADOs):
+    one 2DES point, pulses at 50/150/250 fs, propagated to 300 fs (601 RK4 steps), on
+    the plain bit-exact FP64 path (three trajectories, one stage launch per RK4 stage)
+    and on the FP32-bulk general-size path (the mixed-difference basis, four components).
+    Rates are algorithmic flops (4 [n_ado (16 N^3 + 24 N^2) + 16 N links] per
+    trajectory-step) over host wall time of run_2des (graph replays + read-back)."""
+    from heomtest import rel_err
+
+    text = open(C1_KEY).read()
+    assert "TIME\n0 2000 0.5 0.5" in text
+    d = tempfile.mkdtemp()
+    k = os.path.join(d, "c1_300fs.key")
+    with open(k, "w") as f:
+        f.write(text.replace("TIME\n0 2000 0.5 0.5", "TIME\n0 300 0.5 0.5"))
+    prob = heom.Problem.from_key(k)
+    prob.prepare_sample()
+    shutil.rmtree(d, ignore_errors=True)
+    inf = prob.info
+    depth = prob.ado().astype(int).sum(axis=1)
+    links = 2 * int((depth < inf.L).sum() * inf.K * inf.K_m)
+    F = flops_per_traj_step(inf.sys_size, inf.n_ado, links)
+    steps = steps_of(300.0)
+
+    def timed(plan, **kw):
+        plan.run_2des(**kw)
+        t0 = time.perf_counter()
+        P, _ = plan.run_2des(**kw)
+        return P, time.perf_counter() - t0
+
+    fp64_peak = max(heom.fma_peak_tflops(device, fp64=True) for _ in range(3))
+    px = heom.Plan(prob, "fp64-exact", device=device)
+    Px, tx = timed(px)
+    pb = heom.Plan(prob, "fp32-bulk", device=device)
+    Pb, tb = timed(pb, trajectories=False)
+    ax = F * 3 * steps / tx / 1e12
+    ab = F * 4 * steps / tb / 1e12
+    return {
+        "workload": f"c1 FMO 2DES point: N={inf.sys_size}, {inf.n_ado} ADOs, {links} links, {steps} RK4 steps",
+        "flop_per_trajectory_step": F,
+        "fp64_exact": {"ms_per_step": tx / steps * 1e3, "tflops": ax, "peak_fp64_fma_tflops": fp64_peak,
+                       "frac": ax / fp64_peak,
+                       "note": "three trajectories per step; bit-exact arithmetic uses no FMA, so its "
+                               "ceiling is half the FMA peak; launch: " + px.describe()},
+        "fp32_bulk": {"ms_per_step": tb / steps * 1e3, "tflops": ab, "peak_fp32_fma_tflops": fp32_peak,
+                      "frac": ab / fp32_peak, "rel_err_vs_exact": rel_err(Pb, Px),
+                      "note": "four mixed-difference components per step (general-size staged path)"},
+    }
+
+
 def run_ours(a):
     import torch
 
@@ -323,6 +376,7 @@ def run_ours(a):
         cores = os.cpu_count() or 1
         cpu_val, kind, wall, _ = reference_cpu(rows, cores, cores)
         clocks = clk.summary()
+        large_n = large_n_record(heom, local, peak)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -355,6 +409,7 @@ def run_ours(a):
                              "sample": f"{cores} stratified scan points, one CPU_2DES process each, "
                                        f"{cores} concurrent ({wall:.1f} s)"},
             "clocks": clocks,
+            "large_n": large_n,
         }
         print(json.dumps(out), flush=True)
     if dist:
