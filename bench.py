@@ -423,6 +423,7 @@ def profile_run(precision: str):
 
     fp32-bulk / fp64: the first 148 points of the dimer scan (one per SM) with t3
     shortened to 50 fs, default launch shape, one run of the scan kernel.
+    fp32-bulk-tails: all 1024 points with t3 = 100 fs (the tail kernel's full grid).
     c1-*: one 2DES point of the FMO key (N = 8, 680 ADOs) with the pulses at 10, 20 and
     30 fs (5 fs wide) and the end at 40 fs -- 81 RK4 steps of the general-size staged
     path (c1-fp32-bulk, c1-fp64) or of the bit-exact path (c1-fp64-exact)."""
@@ -454,7 +455,11 @@ def profile_run(precision: str):
         return
     prob = heom.Problem.from_key(KEY)
     prob.prepare_sample()
-    rows = [(a, b, c, c + 50.0) for a, b, c, _ in scan_rows()[:148]]
+    if precision == "fp32-bulk-tails":  # every point, t3 = 100 fs: the tail kernel's full grid
+        rows = [(a, b, c, c + 100.0) for a, b, c, _ in scan_rows()]
+        precision = "fp32-bulk"
+    else:
+        rows = [(a, b, c, c + 50.0) for a, b, c, _ in scan_rows()[:148]]
     plan = heom.Plan(prob, precision, max_points=len(rows))
     r = plan.run_scan(heom.make_points(rows))
     torch.cuda.synchronize()
@@ -467,7 +472,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--profile-run", default=None, choices=["fp32-bulk", "fp64", "c1-fp32-bulk", "c1-fp64", "c1-fp64-exact"],
+    ap.add_argument("--profile-run", default=None, choices=["fp32-bulk", "fp64", "fp32-bulk-tails", "c1-fp32-bulk", "c1-fp64", "c1-fp64-exact"],
                     help="run only a small scan of that precision (for profiler captures)")
     a = ap.parse_args()
     if a.profile_run:
