@@ -950,6 +950,16 @@ int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
     for (int j = 1; j < s.N; j++)
       z = z && Hoff[2 * j] == 0.0 && Hoff[2 * j + 1] == 0.0 && Hoff[2 * j * s.N] == 0.0 && Hoff[2 * j * s.N + 1] == 0.0;
     s.rstat = z;
+    // R = rho_100 starts as |0><0| and feels H, pulse 1 (X0) and the bath (site levels
+    // 1..K).  With H and X0 both zero in column 0 below the diagonal, every term maps a
+    // row-0 matrix to a row-0 matrix, so R stays in row 0; with X3 zero in column 0,
+    // Tr X3 R = sum_l R[0][l] X3[l][0] is then exactly zero.
+    const double *X0 = sys.data() + s.N + 2 * (size_t)s.N * s.N, *X3 = X0 + 6 * (size_t)s.N * s.N;
+    bool r0 = z;
+    for (int j = 0; j < s.N; j++)
+      r0 = r0 && (j == 0 || (X0[2 * j * s.N] == 0.0 && X0[2 * j * s.N + 1] == 0.0)) && X3[2 * j * s.N] == 0.0 &&
+           X3[2 * j * s.N + 1] == 0.0;
+    s.r_row0 = r0;
   }
   cudaError_t e = cudaMemcpyAsync(s.d_sys, sys.data(), sizeof(double) * sys.size(), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -1320,10 +1330,11 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     pl[i] = plan_point(s, tgrid, pts[i]);
     if (pl[i].regular) regular.push_back(i);
   }
-  // three states per regular point: R, D2 at its window start; Q - R at its window end
+  // four states per regular point: R and D2 at its window start; Q - R (or Q) and R at
+  // its window end
   std::vector<long long> snap_of(n, -1);
-  for (size_t k = 0; k < regular.size(); k++) snap_of[regular[k]] = 3 * (long long)k;
-  cudaError_t e = grow<double2>(s.d_snap, s.snap_cap, std::max<size_t>(3 * regular.size(), 1) * snap_elems);
+  for (size_t k = 0; k < regular.size(); k++) snap_of[regular[k]] = 4 * (long long)k;
+  cudaError_t e = grow<double2>(s.d_snap, s.snap_cap, std::max<size_t>(4 * regular.size(), 1) * snap_elems);
   if (e == cudaSuccess) e = grow<int>(s.d_flags, s.flags_cap, (size_t)n + 1); // + the error word
   if (e != cudaSuccess) { s_err = "staged scan snapshots: out of device memory"; return HEOM_ERR_NOMEM; }
   double2 *snap = (double2 *)s.d_snap;
@@ -1335,6 +1346,17 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
 
   struct Keyed { long long key; SlotJob job; std::vector<SlotSave> saves; };
   std::vector<Keyed> q1, q23;
+  // Two-component windows: when pulse 2 is off from D3's wake on, D3 never reaches Q
+  // (dQ = L_123 Q + V3 D2 + V2 D3) nor P (= Tr X3 (Q - R)), and with R in row 0 the
+  // window's records are Tr X3 Q.  Such a window propagates D2 and Q only; stage 1 saves
+  // R at the window's end and the tail kernel forms D = Q - R there.
+  const bool tail_kernel = s.tail_n > 0;
+  std::vector<char> two(n, 0);
+  for (int i : regular) {
+    const PtPlan &q = pl[i];
+    two[i] = tail_kernel && s.r_row0 && q.wD3 != kNever && q.s2 == q.wD3 &&
+             (q.cnt[1] == 0 || q.lo[1] + q.cnt[1] <= q.wD3) && q.s3 < q.nsteps;
+  }
   // stage 1: R and D2 per (tau1, tau2) group up to the members' pulse-3 windows,
   // two groups per job
   std::vector<int> order(regular);
@@ -1343,7 +1365,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     if (pts[a].tau2 != pts[b].tau2) return pts[a].tau2 < pts[b].tau2;
     return pl[a].s2 < pl[b].s2;
   });
-  struct Group { int lead, first, last; std::vector<int> members; };
+  struct Group { int lead, first, last, rlast; std::vector<int> members; }; // rlast: R's last step
   std::vector<Group> groups;
   for (size_t g0 = 0; g0 < order.size();) {
     size_t g1 = g0;
@@ -1358,11 +1380,14 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       G.last = std::max(G.last, pl[order[k]].s2);
     }
     G.first = std::min(std::min(pl[G.lead].wR, pl[G.lead].wD2), G.last);
+    G.rlast = G.last;
+    for (int i : G.members)
+      if (two[i]) G.rlast = std::max(G.rlast, pl[i].s3);
     groups.push_back(G);
     g0 = g1;
   }
   std::sort(groups.begin(), groups.end(),
-            [](const Group &a, const Group &b) { return a.last - a.first > b.last - b.first; });
+            [](const Group &a, const Group &b) { return a.rlast - a.first > b.rlast - b.first; });
   for (size_t g = 0; g < groups.size(); g += 2) {
     Keyed K;
     SlotJob &J = K.job;
@@ -1378,14 +1403,15 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       const PtPlan &q = pl[G.lead];
       set_taus(J, h, pts[G.lead]);
       J.first = std::min(J.first, G.first);
-      J.last = std::max(J.last, G.last);
-      J.slot[2 * h] = slot_mk(1, h, q.wR, G.last, 1, nullptr);
+      J.last = std::max(J.last, G.rlast);
+      J.slot[2 * h] = slot_mk(1, h, q.wR, G.rlast, 1, nullptr);
       J.slot[2 * h + 1] = slot_mk(3, h, q.wD2, G.last, 0, nullptr);
       J.slot[2 * h + 1].src[0] = 2 * h;
       J.slot[2 * h + 1].srcq[0] = 1;
       for (int i : G.members) {
         const int st2 = std::max(pl[i].s2, G.first);
-        K.saves.push_back(SlotSave{st2, 2 * h, -1, -1, 0, 0, state(i, 0)});
+        if (two[i]) K.saves.push_back(SlotSave{pl[i].s3, 2 * h, -1, -1, 0, 0, state(i, 3)}); // R at the end
+        else K.saves.push_back(SlotSave{st2, 2 * h, -1, -1, 0, 0, state(i, 0)});
         K.saves.push_back(SlotSave{st2, 2 * h + 1, -1, i, 1, 0, state(i, 1)});
       }
     }
@@ -1394,8 +1420,52 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     K.key = -1;
     q1.push_back(std::move(K));
   }
-  // stage 2: each point's pulse-3 window (regular points) or the whole point (others)
+  // stage 2: each point's pulse-3 window (regular points) or the whole point (others);
+  // two-component windows two points per job, paired by window start
+  std::vector<int> twos;
+  for (int i : regular)
+    if (two[i]) twos.push_back(i);
+  std::sort(twos.begin(), twos.end(), [&](int a, int b) { return pl[a].s2 != pl[b].s2 ? pl[a].s2 < pl[b].s2 : a < b; });
+  for (size_t k = 0; k < twos.size(); k += 2) {
+    Keyed K;
+    SlotJob &J = K.job;
+    J = SlotJob{};
+    J.first = kNever;
+    J.last = 0;
+    J.wait[0] = J.wait[1] = J.wait[2] = J.wait[3] = -1;
+    J.wait_val = 1;
+    K.key = 0;
+    for (int h = 0; h < 2; h++) {
+      J.slot[2 * h] = J.slot[2 * h + 1] = slot_off();
+      J.rec[2 * h] = J.rec[2 * h + 1] = rec_off();
+      if (k + h >= twos.size()) { set_taus(J, h, pts[twos[k]]); continue; }
+      const int i = twos[k + h];
+      const PtPlan &q = pl[i];
+      set_taus(J, h, pts[i]);
+      J.wait[h] = i;
+      J.first = std::min(J.first, q.s2);
+      J.last = std::max(J.last, q.s3);
+      J.slot[2 * h] = slot_mk(3, h, std::max(q.s2, q.wD2), q.s3, 2, state(i, 1)); // D2: pulse 2 is off
+      J.slot[2 * h + 1] = slot_mk(7, h, std::max(q.s2, q.wQ), q.s3, 0, nullptr);  // Q <- -i[V3, D2]
+      J.slot[2 * h + 1].src[0] = 2 * h;
+      J.slot[2 * h + 1].srcq[0] = 2;
+      SlotRec &r = J.rec[h];
+      r.q = 2 * h + 1;
+      r.r = -1; // Tr X3 R = 0
+      r.first = q.s2;
+      r.last = q.s3;
+      r.rec0 = 0;
+      r.nrec = count_recs(i, q.s2, q.s3);
+      r.tau3 = pts[i].tau3;
+      r.P = P + offsets[i];
+      K.saves.push_back(SlotSave{q.s3, 2 * h + 1, -1, i, 2, 0, state(i, 2)}); // Q at the end
+      K.key = std::max<long long>(K.key, q.s2);
+    }
+    std::stable_sort(K.saves.begin(), K.saves.end(), [](const SlotSave &a, const SlotSave &b) { return a.step < b.step; });
+    q23.push_back(std::move(K));
+  }
   for (int i = 0; i < n; i++) {
+    if (two[i]) continue;
     const PtPlan &q = pl[i];
     const bool reg = q.regular;
     Keyed K;
@@ -1443,7 +1513,6 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   std::sort(tails.begin(), tails.end(), [&](int a, int b) {
     return pl[a].s3 != pl[b].s3 ? pl[a].s3 < pl[b].s3 : pl[a].nsteps < pl[b].nsteps;
   });
-  const bool tail_kernel = s.tail_n > 0;
   for (size_t k = 0; k < (tail_kernel ? 0 : tails.size()); k += 4) {
     Keyed K;
     SlotJob &J = K.job;
@@ -1547,6 +1616,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       T.pad = 0;
       T.tau3 = pts[i].tau3;
       T.init = state(i, 2);
+      T.minus = two[i] ? state(i, 3) : nullptr; // D = Q - R at the window end
       T.P = P + offsets[i];
       tail_work += q.nsteps - q.s3;
     }

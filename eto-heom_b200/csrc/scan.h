@@ -45,6 +45,7 @@ struct ScanState {
   // pulse-free tails two points per CTA
   bool staged = false;           // chosen for heom_run_scan / heom_run_scan_device
   bool rstat = false;            // H couples level 0 to nothing (|0><0| stationary)
+  bool r_row0 = false;           // R stays in row 0 and Tr X3 R = 0 (see scan_upload_system)
   int sl_threads = 0, sl_grid = 0, sl_wcap = 0;
   size_t sl_smem = 0;
   void *d_snap = nullptr;        // snapshots: 2 states per regular point
