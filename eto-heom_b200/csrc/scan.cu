@@ -1330,11 +1330,11 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     pl[i] = plan_point(s, tgrid, pts[i]);
     if (pl[i].regular) regular.push_back(i);
   }
-  // four states per regular point: R and D2 at its window start; Q - R (or Q) and R at
-  // its window end
+  // three states per regular point: R and D2 at its window start; the tail's initial
+  // state at its window end
   std::vector<long long> snap_of(n, -1);
-  for (size_t k = 0; k < regular.size(); k++) snap_of[regular[k]] = 4 * (long long)k;
-  cudaError_t e = grow<double2>(s.d_snap, s.snap_cap, std::max<size_t>(4 * regular.size(), 1) * snap_elems);
+  for (size_t k = 0; k < regular.size(); k++) snap_of[regular[k]] = 3 * (long long)k;
+  cudaError_t e = grow<double2>(s.d_snap, s.snap_cap, std::max<size_t>(3 * regular.size(), 1) * snap_elems);
   if (e == cudaSuccess) e = grow<int>(s.d_flags, s.flags_cap, (size_t)n + 1); // + the error word
   if (e != cudaSuccess) { s_err = "staged scan snapshots: out of device memory"; return HEOM_ERR_NOMEM; }
   double2 *snap = (double2 *)s.d_snap;
@@ -1346,16 +1346,16 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
 
   struct Keyed { long long key; SlotJob job; std::vector<SlotSave> saves; };
   std::vector<Keyed> q1, q23;
-  // Two-component windows: when pulse 2 is off from D3's wake on, D3 never reaches Q
-  // (dQ = L_123 Q + V3 D2 + V2 D3) nor P (= Tr X3 (Q - R)), and with R in row 0 the
-  // window's records are Tr X3 Q.  Such a window propagates D2 and Q only; stage 1 saves
-  // R at the window's end and the tail kernel forms D = Q - R there.
+  // With R in row 0 and Tr X3 R = 0 (s.r_row0), P = Tr X3 Q, and the tail (no pulse on,
+  // so R and Q evolve apart) starts from Q; R is then needed only as a source: of D2 in
+  // pulse 2's window and of D3 in pulse 3's.  Two-component windows: when pulse 2 is off
+  // from D3's wake on, D3 never reaches Q (dQ = L_123 Q + V3 D2 + V2 D3) nor P, so such a
+  // window propagates D2 and Q only and needs no R.
   const bool tail_kernel = s.tail_n > 0;
   std::vector<char> two(n, 0);
   for (int i : regular) {
     const PtPlan &q = pl[i];
-    two[i] = tail_kernel && s.r_row0 && q.wD3 != kNever && q.s2 == q.wD3 &&
-             (q.cnt[1] == 0 || q.lo[1] + q.cnt[1] <= q.wD3) && q.s3 < q.nsteps;
+    two[i] = s.r_row0 && q.wD3 != kNever && q.s2 == q.wD3 && (q.cnt[1] == 0 || q.lo[1] + q.cnt[1] <= q.wD3);
   }
   // stage 1: R and D2 per (tau1, tau2) group up to the members' pulse-3 windows,
   // two groups per job
@@ -1381,13 +1381,18 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     }
     G.first = std::min(std::min(pl[G.lead].wR, pl[G.lead].wD2), G.last);
     G.rlast = G.last;
-    for (int i : G.members)
-      if (two[i]) G.rlast = std::max(G.rlast, pl[i].s3);
+    if (s.r_row0) { // R until pulse 2's window closes and the four-component windows start
+      const PtPlan &q = pl[G.lead];
+      G.rlast = q.cnt[1] > 0 ? q.lo[1] + q.cnt[1] : 0;
+      for (int i : G.members)
+        if (!two[i]) G.rlast = std::max(G.rlast, std::max(pl[i].s2, G.first));
+      G.rlast = std::min(G.rlast, G.last);
+    }
     groups.push_back(G);
     g0 = g1;
   }
   std::sort(groups.begin(), groups.end(),
-            [](const Group &a, const Group &b) { return a.rlast - a.first > b.rlast - b.first; });
+            [](const Group &a, const Group &b) { return a.last - a.first > b.last - b.first; });
   for (size_t g = 0; g < groups.size(); g += 2) {
     Keyed K;
     SlotJob &J = K.job;
@@ -1403,15 +1408,14 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       const PtPlan &q = pl[G.lead];
       set_taus(J, h, pts[G.lead]);
       J.first = std::min(J.first, G.first);
-      J.last = std::max(J.last, G.rlast);
+      J.last = std::max(J.last, G.last);
       J.slot[2 * h] = slot_mk(1, h, q.wR, G.rlast, 1, nullptr);
       J.slot[2 * h + 1] = slot_mk(3, h, q.wD2, G.last, 0, nullptr);
       J.slot[2 * h + 1].src[0] = 2 * h;
       J.slot[2 * h + 1].srcq[0] = 1;
       for (int i : G.members) {
         const int st2 = std::max(pl[i].s2, G.first);
-        if (two[i]) K.saves.push_back(SlotSave{pl[i].s3, 2 * h, -1, -1, 0, 0, state(i, 3)}); // R at the end
-        else K.saves.push_back(SlotSave{st2, 2 * h, -1, -1, 0, 0, state(i, 0)});
+        if (!two[i]) K.saves.push_back(SlotSave{st2, 2 * h, -1, -1, 0, 0, state(i, 0)});
         K.saves.push_back(SlotSave{st2, 2 * h + 1, -1, i, 1, 0, state(i, 1)});
       }
     }
@@ -1501,7 +1505,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     J.rec[0].tau3 = pts[i].tau3;
     J.rec[0].P = P + offsets[i];
     J.rec[1] = J.rec[2] = J.rec[3] = rec_off();
-    if (reg) K.saves.push_back(SlotSave{J.last, 3, 0, i, 2, 0, state(i, 2)}); // Q - R
+    if (reg) K.saves.push_back(SlotSave{J.last, 3, s.r_row0 ? -1 : 0, i, 2, 0, state(i, 2)}); // Q or Q - R
     K.key = reg ? q.s2 : 0;
     q23.push_back(std::move(K));
   }
@@ -1616,7 +1620,6 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       T.pad = 0;
       T.tau3 = pts[i].tau3;
       T.init = state(i, 2);
-      T.minus = two[i] ? state(i, 3) : nullptr; // D = Q - R at the window end
       T.P = P + offsets[i];
       tail_work += q.nsteps - q.s3;
     }

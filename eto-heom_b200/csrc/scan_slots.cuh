@@ -598,8 +598,7 @@ struct TailPoint {
   int first, last;       // steps [s3, end) of the point
   int rec0, pad;         // index of its first record in P
   double tau3;
-  const double2 *init;   // D at s3, [NN][n_ado] (or Q, when minus is set)
-  const double2 *minus;  // R at s3 (D = init - minus), or nullptr
+  const double2 *init;   // the tail's state at s3 (D = Q - R, or Q), [NN][n_ado]
   double2 *P;            // the point's output
 };
 
@@ -685,14 +684,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) scan_tail(TailArgs a) {
     const size_t pos = e / ((size_t)G * nado), rest = e - pos * G * nado;
     const int p2 = (int)(rest / nado), n2 = (int)(rest - (size_t)p2 * nado);
     double2 v = make_double2(0.0, 0.0);
-    if (gbase + p2 < a.n_pts) {
-      const size_t off = (size_t)(int)a.tail[1 + pos] * nado + n2;
-      v = __ldcg(a.pts[gbase + p2].init + off);
-      if (a.pts[gbase + p2].minus) { // the slot kernel's FP64 difference of two states
-        const double2 u = __ldcg(a.pts[gbase + p2].minus + off);
-        v = make_double2(v.x - u.x, v.y - u.y);
-      }
-    }
+    if (gbase + p2 < a.n_pts) v = __ldcg(a.pts[gbase + p2].init + (size_t)(int)a.tail[1 + pos] * nado + n2);
     rho[e] = v;
     w32[e] = mk2<T>(v.x, v.y);
     w32[cells + e] = mk2<T>(v.x, v.y);
