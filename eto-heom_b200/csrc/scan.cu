@@ -1176,6 +1176,7 @@ SlotFn slot_kernel(int precision) {
   return precision == HEOM_FP64 ? scan_slots<double, 4, kSlotThreads> : scan_slots<float, 4, kSlotThreads>;
 }
 constexpr int kNever = 0x7fffffff;
+constexpr int kSoloGroups = 64; // stage-1 groups (longest first) that get a job of their own
 
 // Per-point schedule, with the kernels' float time grid and window tests.
 struct PtPlan {
@@ -1393,7 +1394,9 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   }
   std::sort(groups.begin(), groups.end(),
             [](const Group &a, const Group &b) { return a.last - a.first > b.last - b.first; });
-  for (size_t g = 0; g < groups.size(); g += 2) {
+  const size_t solo = std::min<size_t>(groups.size(), (size_t)std::max(0, kSoloGroups));
+  for (size_t g = 0; g < groups.size(); g += g < solo ? 1 : 2) {
+    const size_t ng = g < solo ? 1 : 2; // the longest groups alone: they set the critical path
     Keyed K;
     SlotJob &J = K.job;
     J = SlotJob{};
@@ -1403,7 +1406,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     for (int r = 0; r < 4; r++) J.rec[r] = rec_off();
     for (int h = 0; h < 2; h++) {
       J.slot[2 * h] = J.slot[2 * h + 1] = slot_off();
-      if (g + h >= groups.size()) { set_taus(J, h, pts[groups[g].lead]); continue; }
+      if (h >= (int)ng || g + h >= groups.size()) { set_taus(J, h, pts[groups[g].lead]); continue; }
       const Group &G = groups[g + h];
       const PtPlan &q = pl[G.lead];
       set_taus(J, h, pts[G.lead]);
