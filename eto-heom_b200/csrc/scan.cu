@@ -39,6 +39,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <complex>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -933,6 +934,8 @@ static void tail_table(const std::vector<double> &sys, int N, std::vector<double
   }
 }
 
+static void dual_operator(ScanState &s, const std::vector<double> &sys, const std::vector<double> &tab);
+
 int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
   if (!s.supported) return 0;
   std::vector<double> sys;
@@ -943,6 +946,7 @@ int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
     s.tail_n = (int)tab[0];
     cudaError_t e = cudaMemcpyAsync(s.d_tail, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) { s_err = std::string("tail table upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+    if (s.tail_n > 0) dual_operator(s, sys, tab);
   }
   { // the kernels' test for a stationary |0><0| (off-diagonal H in row and column 0)
     const double *Hoff = sys.data() + s.N;
@@ -1312,6 +1316,129 @@ template <class T> static cudaError_t grow(void *&ptr, size_t &cap, size_t want)
   return e;
 }
 
+// Dual tails.  The pulse-free operator on the reduced cells (cell = e * n_ado + n:
+// position e of the tail table, ADO n in the kernels' order), in FP64, as the tail
+// arithmetic defines it: -i C z (the restricted commutator), the bath links of the
+// cell's site row r and site column c, and (damping + i (damping' - (H_rr - H_cc))) z.
+// Kept transposed (CSR of L^T) with the readout vector x3 (Tr X3 . on ADO 0) as w_0.
+static void dual_operator(ScanState &s, const std::vector<double> &sys, const std::vector<double> &tab) {
+  const int ne = (int)tab[0], nado = s.n_ado, K = s.K, Km = s.K_m, N = s.N, NN = N * N, cells = ne * nado;
+  const TableLayout tl(nado, s.M, Km);
+  const PmLinkHost *L = (const PmLinkHost *)(s.h_tables.data() + tl.plink);
+  const double *dmp = (const double *)(s.h_tables.data() + tl.pdamp);
+  const double *Hd = sys.data(), *X3 = sys.data() + N + 2 * NN + 6 * NN;
+  const double *C = tab.data() + 1 + kTailMax;
+  std::vector<std::vector<std::pair<int, std::complex<double>>>> lt(cells); // lt[c'] : (c, L[c][c'])
+  s.dual_diag.assign(2 * (size_t)cells, 0.0);
+  auto add = [&](int c, int c2, std::complex<double> v) { lt[c2].push_back({c, v}); };
+  const std::complex<double> I(0.0, 1.0);
+  for (int e = 0; e < ne; e++) {
+    const int q = (int)tab[1 + e], r = q / N, c = q - r * N;
+    for (int n = 0; n < nado; n++) {
+      const int cell = e * nado + n;
+      for (int f = 0; f < ne; f++) {
+        const std::complex<double> cf(C[2 * (e * kTailMax + f)], C[2 * (e * kTailMax + f) + 1]);
+        if (cf != 0.0) add(cell, f * nado + n, -I * cf);
+      }
+      if (r >= 1 && r <= K)
+        for (int k = 0; k < Km; k++) {
+          const PmLinkHost &l = L[(size_t)((r - 1) + k * K) * nado + n];
+          const unsigned u = (unsigned)l.ud & 0xffffu, d = (unsigned)l.ud >> 16;
+          if (u != 0xffffu && c != r) add(cell, e * nado + (int)u, I * l.x);
+          if (d != 0xffffu) add(cell, e * nado + (int)d, std::complex<double>(c == r ? -2 * l.by : -l.by, c == r ? 0.0 : l.ay));
+        }
+      if (c >= 1 && c <= K && c != r)
+        for (int k = 0; k < Km; k++) {
+          const PmLinkHost &l = L[(size_t)((c - 1) + k * K) * nado + n];
+          const unsigned u = (unsigned)l.ud & 0xffffu, d = (unsigned)l.ud >> 16;
+          if (u != 0xffffu) add(cell, e * nado + (int)u, -I * l.x);
+          if (d != 0xffffu) add(cell, e * nado + (int)d, std::complex<double>(-l.by, -l.ay));
+        }
+      s.dual_diag[2 * cell] = dmp[2 * n];
+      s.dual_diag[2 * cell + 1] = dmp[2 * n + 1] - (Hd[r] - Hd[c]);
+    }
+  }
+  s.dual_start.assign(cells + 1, 0);
+  s.dual_idx.clear();
+  s.dual_coef.clear();
+  for (int c2 = 0; c2 < cells; c2++) {
+    s.dual_start[c2] = (int)s.dual_idx.size();
+    for (const auto &t : lt[c2]) {
+      s.dual_idx.push_back(t.first);
+      s.dual_coef.push_back(t.second.real());
+      s.dual_coef.push_back(t.second.imag());
+    }
+  }
+  s.dual_start[cells] = (int)s.dual_idx.size();
+  s.h_W.assign(2 * (size_t)cells, 0.0); // w_0 = x3: P = sum_e X3[c][r] Q[e][ADO 0]
+  for (int e = 0; e < ne; e++) {
+    const int q = (int)tab[1 + e], r = q / N, c = q - r * N;
+    s.h_W[2 * ((size_t)e * nado + s.ado0)] = X3[2 * (c * N + r)];
+    s.h_W[2 * ((size_t)e * nado + s.ado0) + 1] = X3[2 * (c * N + r) + 1];
+  }
+  s.W_rows = 1;
+  s.W_dev_rows = 0;
+  s.dual_pos.assign(ne, 0);
+  for (int e = 0; e < ne; e++) s.dual_pos[e] = (int)tab[1 + e];
+  s.dual_pos_dirty = true;
+}
+
+// Extend the dual vectors to `rows` (w_{k+1} = T4(h L^T) w_k in Horner form, FP64) and
+// bring them to the device.
+static int dual_rows(ScanState &s, int rows, cudaStream_t st) {
+  const int cells = s.tail_n * s.n_ado;
+  if (s.W_rows < rows) {
+    s.h_W.resize(2 * (size_t)cells * rows);
+    std::vector<double> u(2 * (size_t)cells), lu(2 * (size_t)cells);
+    const double *D = s.dual_diag.data(), *Cf = s.dual_coef.data();
+    for (int k = s.W_rows; k < rows; k++) {
+      const double *w = s.h_W.data() + 2 * (size_t)cells * (k - 1);
+      std::copy(w, w + 2 * (size_t)cells, u.begin());
+      for (int m = 4; m >= 1; m--) { // u = w + (h/m) L^T u (complex arithmetic written out)
+        for (int c2 = 0; c2 < cells; c2++) {
+          double ar = D[2 * c2] * u[2 * c2] - D[2 * c2 + 1] * u[2 * c2 + 1];
+          double ai = D[2 * c2] * u[2 * c2 + 1] + D[2 * c2 + 1] * u[2 * c2];
+          for (int j = s.dual_start[c2]; j < s.dual_start[c2 + 1]; j++) {
+            const double *z = u.data() + 2 * (size_t)s.dual_idx[j];
+            ar += Cf[2 * j] * z[0] - Cf[2 * j + 1] * z[1];
+            ai += Cf[2 * j] * z[1] + Cf[2 * j + 1] * z[0];
+          }
+          lu[2 * c2] = ar;
+          lu[2 * c2 + 1] = ai;
+        }
+        const double cm = s.h / m;
+        for (size_t c = 0; c < 2 * (size_t)cells; c++) u[c] = w[c] + cm * lu[c];
+      }
+      std::copy(u.begin(), u.end(), s.h_W.begin() + 2 * (size_t)cells * k);
+    }
+    s.W_rows = rows;
+  }
+  cudaError_t e = cudaSuccess;
+  const size_t row_bytes = sizeof(double2) * (size_t)cells;
+  if ((size_t)rows * row_bytes > s.W_cap) {
+    if (s.d_W) cudaFree(s.d_W);
+    s.d_W = nullptr;
+    s.W_cap = 0;
+    s.W_dev_rows = 0;
+    e = cudaMalloc(&s.d_W, (size_t)rows * row_bytes);
+    if (e == cudaSuccess) s.W_cap = (size_t)rows * row_bytes;
+  }
+  if (e == cudaSuccess && s.W_dev_rows < rows) {
+    e = cudaMemcpyAsync((unsigned char *)s.d_W + s.W_dev_rows * row_bytes, s.h_W.data() + 2 * (size_t)cells * s.W_dev_rows,
+                        (rows - s.W_dev_rows) * row_bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st); // the host rows may be reallocated later
+    if (e == cudaSuccess) s.W_dev_rows = rows;
+  }
+  if (e == cudaSuccess && s.dual_pos_dirty) {
+    if (!s.d_dualpos) e = cudaMalloc(&s.d_dualpos, sizeof(int) * kTailMax);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(s.d_dualpos, s.dual_pos.data(), sizeof(int) * s.dual_pos.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) s.dual_pos_dirty = false;
+  }
+  if (e != cudaSuccess) { s_err = std::string("dual tail rows: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  return 0;
+}
+
 int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, const long long *offsets,
                cudaStream_t st) {
   const int NN = s.N * s.N;
@@ -1605,66 +1732,49 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   if (e != cudaSuccess) { s_err = std::string("staged scan launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
   s.staged_launches++;
   s.err_pending = (int *)s.d_flags + n;
-  long long tail_work = 0;
   if (tail_kernel && !tails.empty()) {
-    // G points per CTA on the reduced positions, at least one CTA per SM when possible
-    const int per_cta = std::max(1, kTailThreads / s.n_ado);
-    const int G = std::max(1, std::min(per_cta, (int)((tails.size() + s.sm_count - 1) / s.sm_count)));
-    const int nblk = (int)((tails.size() + G - 1) / G);
-    std::vector<TailPoint> tp(tails.size());
-    std::vector<float> tfirst(nblk);
-    for (size_t k = 0; k < tails.size(); k++) {
-      const int i = tails[k];
+    // records w_k^T q of every tail (scan_tail_dual), G points per CTA
+    int kmax = 0;
+    std::vector<DualPoint> dp;
+    dp.reserve(tails.size());
+    for (int i : tails) {
       const PtPlan &q = pl[i];
-      TailPoint &T = tp[k];
-      T.first = q.s3;
-      T.last = q.nsteps;
-      T.rec0 = records_before(s, q, q.s3);
-      T.pad = 0;
-      T.tau3 = pts[i].tau3;
-      T.init = state(i, 2);
-      T.P = P + offsets[i];
-      tail_work += q.nsteps - q.s3;
+      const int rec0 = records_before(s, q, q.s3), cnt = records_before(s, q, q.nsteps) - rec0;
+      if (cnt <= 0) continue;
+      // first record at or after s3: records fall on rs + j * stride
+      const int r1 = q.s3 <= q.rs ? q.rs : q.rs + (q.s3 - q.rs + s.stride - 1) / s.stride * s.stride;
+      DualPoint d;
+      d.q = state(i, 2);
+      d.P = P + offsets[i] + rec0;
+      d.k0 = r1 - q.s3;
+      d.count = cnt;
+      kmax = std::max(kmax, d.k0 + (cnt - 1) * s.stride + 1);
+      dp.push_back(d);
     }
-    for (int b = 0; b < nblk; b++) {
-      int f = kNever;
-      for (int k = b * G; k < std::min((int)tails.size(), (b + 1) * G); k++) f = std::min(f, tp[k].first);
-      tfirst[b] = s.t_grid[f];
+    if (!dp.empty()) {
+      int rc = dual_rows(s, kmax, st);
+      if (rc) return rc;
+      e = grow<DualPoint>(s.d_tailpts, s.tailpts_cap, dp.size());
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s.d_tailpts, dp.data(), sizeof(DualPoint) * dp.size(), cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess) { s_err = std::string("tail upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+      DualArgs da{};
+      da.ne = s.tail_n;
+      da.nado = s.n_ado;
+      da.stride = s.stride;
+      da.n_pts = (int)dp.size();
+      da.pos = (const int *)s.d_dualpos;
+      da.W = (const double2 *)s.d_W;
+      da.pts = (const DualPoint *)s.d_tailpts;
+      const size_t smem = sizeof(double2) * (size_t)kDualG * s.tail_n * s.n_ado;
+      e = cudaFuncSetAttribute(scan_tail_dual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess) {
+        scan_tail_dual<<<(int)((dp.size() + kDualG - 1) / kDualG), kDualThreads, smem, st>>>(da);
+        e = cudaGetLastError();
+      }
+      if (e != cudaSuccess) { s_err = std::string("tail launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+      s.staged_launches++;
     }
-    e = grow<TailPoint>(s.d_tailpts, s.tailpts_cap, tp.size());
-    if (e == cudaSuccess) e = grow<float>(s.d_tfirst, s.tfirst_cap, tfirst.size());
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(s.d_tailpts, tp.data(), sizeof(TailPoint) * tp.size(), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(s.d_tfirst, tfirst.data(), sizeof(float) * tfirst.size(), cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) { s_err = std::string("tail upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
-    TailArgs ta{};
-    ta.N = s.N;
-    ta.n_ado = s.n_ado;
-    ta.M = s.M;
-    ta.K = s.K;
-    ta.K_m = s.K_m;
-    ta.stride = s.stride;
-    ta.ado0 = s.ado0;
-    ta.n_pts = (int)tp.size();
-    ta.G = G;
-    ta.dt = s.dt;
-    ta.h = s.h;
-    ta.tables = (const unsigned char *)s.d_tables;
-    ta.sys = s.d_sys;
-    ta.tail = (const double *)s.d_tail;
-    ta.pts = (const TailPoint *)s.d_tailpts;
-    ta.t_first = (const float *)s.d_tfirst;
-    const size_t tsz = s.precision == HEOM_FP64 ? 8 : 4;
-    const size_t smem = tail_smem_bytes<4>(tsz, s.n_ado, s.M, G, s.tail_n);
-    auto tk = s.precision == HEOM_FP64 ? scan_tail<double, 4> : scan_tail<float, 4>;
-    e = cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) {
-      tk<<<nblk, (G * s.n_ado + 31) / 32 * 32, smem, st>>>(ta);
-      e = cudaGetLastError();
-    }
-    if (e != cudaSuccess) { s_err = std::string("tail launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
-    s.staged_launches++;
   }
   s.last_work = 0;
   for (const SlotJob &J : jobs) { // propagated component-steps (a reduced step counts its share)
@@ -1672,7 +1782,6 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     for (const SlotSpec &z : J.slot) w += std::max(0, std::min(z.stop, J.last) - std::max(z.wake, J.first));
     s.last_work += J.mode == 1 ? w * s.tail_n / (s.N * s.N) : w;
   }
-  s.last_work += tail_work * s.tail_n / (s.N * s.N);
   return 0;
 }
 
@@ -1693,6 +1802,7 @@ int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_point
               bool single_pass) {
   std::vector<unsigned char> tb;
   if (!scan_prepare(s, p, precision, max_points, tb)) return 0; // unsupported: s.why says why
+  s.h_tables = tb; // host copy: the dual tails are built from the links and damping
   if (!single_pass) staged_prepare(s);
   cudaError_t e = cudaMalloc(&s.d_tables, s.tables_bytes);
   if (e == cudaSuccess) e = cudaMemcpy(s.d_tables, tb.data(), s.tables_bytes, cudaMemcpyHostToDevice);
@@ -1801,7 +1911,8 @@ void scan_release(ScanState &s) {
   if (s.d_flags) cudaFree(s.d_flags);
   if (s.d_tail) cudaFree(s.d_tail);
   if (s.d_tailpts) cudaFree(s.d_tailpts);
-  if (s.d_tfirst) cudaFree(s.d_tfirst);
+  if (s.d_W) cudaFree(s.d_W);
+  if (s.d_dualpos) cudaFree(s.d_dualpos);
   if (s.d_jobs) cudaFree(s.d_jobs);
   if (s.d_saves) cudaFree(s.d_saves);
   if (s.d_tables) cudaFree(s.d_tables);

@@ -57,8 +57,17 @@ struct ScanState {
   std::vector<float> t_grid;     // float time of each step (t_start + dt accumulated)
   void *d_tail = nullptr;        // reduced-tail table of the current sample
   int tail_n = 0;                // its positions (0: tails run on full blocks)
-  void *d_tailpts = nullptr, *d_tfirst = nullptr; // the tail kernel's points and start times
-  size_t tailpts_cap = 0, tfirst_cap = 0;
+  void *d_tailpts = nullptr;     // the tail kernel's points
+  size_t tailpts_cap = 0;
+  // dual tails (scan_tail_dual): L^T of the pulse-free reduced system (CSR) and its
+  // diagonal, w_k rows on the host and the device, the reduced positions
+  std::vector<unsigned char> h_tables;
+  std::vector<int> dual_start, dual_idx, dual_pos;
+  std::vector<double> dual_coef, dual_diag, h_W;
+  int W_rows = 0, W_dev_rows = 0;
+  bool dual_pos_dirty = false;
+  void *d_W = nullptr, *d_dualpos = nullptr;
+  size_t W_cap = 0;
   std::vector<heom_scan_point> rb_pts; // points / offsets read back for heom_run_scan_device
   std::vector<long long> rb_off;
   long long staged_launches = 0;

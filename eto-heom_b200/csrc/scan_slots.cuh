@@ -587,218 +587,62 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
 }
 
 // ------------------------------------------------------------------ tail kernel
-// The pulse-free tails of a staged scan, after the slot kernel: D = Q - R of G points per
-// CTA on the reduced positions only (see tail_doubles).  Nothing depends on time once
-// every pulse is off, so a step is four Horner stages with no set-up; the owner of ADO 0
-// of each point writes P = Tr X3 D itself.  Shared layout [position e][point p][ADO n].
+// The pulse-free tails of a staged scan, after the slot kernel.  Once every pulse is off
+// the step map is one fixed matrix T = sum_{j<=4} (hL)^j / j! (L: the pulse-free HEOM
+// operator on the reduced positions, see tail_doubles), the same for every point, so
+// the tail records of a point with state q at its window end s3 are
+//   P(s3 + k) = x3^T T^k q = w_k^T q,   w_k = (T^T)^k x3,
+// x3 the readout (Tr X3 . on ADO 0).  The host propagates the dual vectors w_k once per
+// sample in FP64; here each record is one FP64 dot product over the reduced cells.
+// One warp per record, G points per CTA sharing the rows of w.
 
-constexpr int kTailThreads = 512;
+constexpr int kDualG = 4;        // points per CTA
+constexpr int kDualThreads = 256;
 
-struct TailPoint {
-  int first, last;       // steps [s3, end) of the point
-  int rec0, pad;         // index of its first record in P
-  double tau3;
-  const double2 *init;   // the tail's state at s3 (D = Q - R, or Q), [NN][n_ado]
-  double2 *P;            // the point's output
+struct DualPoint {
+  const double2 *q;  // the point's state at s3, [NN][n_ado] (Q, or Q - R)
+  double2 *P;        // its first tail record
+  int k0, count;     // records at k = k0 + j * stride, j < count
 };
 
-struct TailArgs {
-  int N, n_ado, M, K, K_m, stride, ado0, n_pts, G;
-  float dt;
-  double h;
-  const unsigned char *tables;
-  const double *sys;
-  const double *tail;    // the reduced-tail table
-  const TailPoint *pts;  // G per CTA, ordered by first step
-  const float *t_first;  // float time at each CTA's first step
+struct DualArgs {
+  int ne, nado, stride, n_pts;
+  const int *pos;        // the reduced positions (r * N + c)
+  const double2 *W;      // w_k, [k][cell], cell = e * nado + n
+  const DualPoint *pts;
 };
 
-template <int NT> __host__ __device__ inline size_t tail_smem_bytes(size_t tsz, int n_ado, int M, int G, int ne) {
-  const size_t cells = (size_t)ne * G * n_ado;
-  size_t b = 0;
-  b += al16(16 * cells);                // rho (FP64)
-  b += al16(2 * 2 * tsz * cells);       // w copies, double-buffered
-  b += al16((tsz == 4 ? 16 : 32) * (size_t)n_ado * M); // links
-  b += al16(16 * (size_t)n_ado);        // damping scalars
-  return b;
-}
-
-template <typename T, int NT>
-__global__ void __launch_bounds__(kTailThreads, 1) scan_tail(TailArgs a) {
-  using T2 = typename V2<T>::t;
-  constexpr int NN = NT * NT;
+__global__ void __launch_bounds__(kDualThreads) scan_tail_dual(DualArgs a) {
   extern __shared__ __align__(16) unsigned char sm[];
-  __shared__ int s_pos[kTailMax], s_ne;
-  __shared__ unsigned s_mask[kTailMax];
-  __shared__ T2 s_C[kTailMax * kTailMax];
-  __shared__ double s_gi[kTailMax];      // -(H_rr - H_cc) of each position
-  __shared__ double2 s_x3[kTailMax];     // X3[c][r] of each position (the trace weight)
-  const int nado = a.n_ado, M = a.M, K = a.K, Km = a.K_m, G = a.G;
-  const int tid = threadIdx.x, bs = blockDim.x;
-  const int ne = (int)a.tail[0];
-  const size_t cells = (size_t)ne * G * nado, nM = (size_t)nado * M;
-  unsigned char *p = sm;
-  double2 *rho = (double2 *)p;
-  p += al16(16 * cells);
-  T2 *w32 = (T2 *)p; // [2][ne][G][nado]
-  p += al16(2 * sizeof(T2) * cells);
-  PmLink<T> *links = (PmLink<T> *)p;
-  p += al16(sizeof(PmLink<T>) * nM);
-  double2 *sdamp = (double2 *)p;
-  TableLayout tl(nado, M, Km);
-  const PmLinkHost *g_link = (const PmLinkHost *)(a.tables + tl.plink);
-  const double2 *g_damp = (const double2 *)(a.tables + tl.pdamp);
-  for (size_t q = tid; q < nM; q += bs) {
-    const PmLinkHost L = g_link[q];
-    PmLink<T> v;
-    v.x = (T)L.x;
-    v.by = (T)L.by;
-    v.ay = (T)L.ay;
-    v.ud = L.ud;
-    links[q] = v;
-  }
-  for (int q = tid; q < nado; q += bs) sdamp[q] = g_damp[q];
-  const double *g_Hd = a.sys, *g_X3 = a.sys + NT + 2 * NN + 6 * NN;
-  if (tid == 0) s_ne = ne;
-  if (tid < kTailMax) {
-    const int q = tid < ne ? (int)a.tail[1 + tid] : 0, r = q / NT, c = q - r * NT;
-    s_pos[tid] = q;
-    s_gi[tid] = -(g_Hd[r] - g_Hd[c]);
-    s_x3[tid] = make_double2(g_X3[2 * (c * NT + r)], g_X3[2 * (c * NT + r) + 1]);
-    unsigned m = 0;
-    for (int f = 0; f < kTailMax; f++) {
-      const double cr = a.tail[1 + kTailMax + 2 * (tid * kTailMax + f)];
-      const double ci = a.tail[1 + kTailMax + 2 * (tid * kTailMax + f) + 1];
-      s_C[tid * kTailMax + f] = mk2<T>(cr, ci);
-      if (cr != 0.0 || ci != 0.0) m |= 1u << f;
-    }
-    s_mask[tid] = m;
-  }
-  // this thread: ADO n of point pp of the CTA's group
-  const int pp = tid / nado, n = tid - pp * nado;
-  const int gbase = blockIdx.x * G;
-  const bool mine = pp < G && gbase + pp < a.n_pts;
-  const TailPoint me = a.pts[mine ? gbase + pp : 0];
-  // initial states
-  for (size_t e = tid; e < cells; e += bs) {
-    const size_t pos = e / ((size_t)G * nado), rest = e - pos * G * nado;
-    const int p2 = (int)(rest / nado), n2 = (int)(rest - (size_t)p2 * nado);
-    double2 v = make_double2(0.0, 0.0);
-    if (gbase + p2 < a.n_pts) v = __ldcg(a.pts[gbase + p2].init + (size_t)(int)a.tail[1 + pos] * nado + n2);
-    rho[e] = v;
-    w32[e] = mk2<T>(v.x, v.y);
-    w32[cells + e] = mk2<T>(v.x, v.y);
+  double2 *q = (double2 *)sm; // [G][cells]
+  __shared__ DualPoint s_pt[kDualG];
+  const int cells = a.ne * a.nado, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int p0 = blockIdx.x * kDualG, G = min(kDualG, a.n_pts - p0);
+  if (tid < G) s_pt[tid] = a.pts[p0 + tid];
+  __syncthreads();
+  for (int t = tid; t < G * cells; t += blockDim.x) {
+    const int g = t / cells, c = t - g * cells, e = c / a.nado, n = c - e * a.nado;
+    q[t] = __ldcg(s_pt[g].q + (size_t)a.pos[e] * a.nado + n);
   }
   __syncthreads();
-  int first = 0x7fffffff, last = 0;
-  for (int k = 0; k < G && gbase + k < a.n_pts; k++) {
-    first = min(first, a.pts[gbase + k].first);
-    last = max(last, a.pts[gbase + k].last);
-  }
-  const double2 dmp = sdamp[n];
-  const size_t pstride = (size_t)G * nado; // between positions
-  const int blk = pp * nado + n;           // within a position
-  float t = a.t_first[blockIdx.x];
-  int rec = 0, buf = 0;
-  for (int i = first; i < last; i++) {
-    const bool live = mine && i >= me.first && i < me.last;
-    double2 w64[kTailMax];
-#pragma unroll
-    for (int e = 0; e < kTailMax; e++)
-      w64[e] = (live && e < ne) ? rho[e * pstride + blk] : make_double2(0.0, 0.0);
-    if (live && n == a.ado0 && t >= me.tau3 && i % a.stride == 0) { // P before the step
-      double pr = 0.0, pi = 0.0;
-#pragma unroll
-      for (int e = 0; e < kTailMax; e++) {
-        if (e >= ne) break;
-        const double2 x = s_x3[e], v = w64[e];
-        pr += v.x * x.x - v.y * x.y;
-        pi += v.x * x.y + v.y * x.x;
+  int jmax = 0;
+  for (int g = 0; g < G; g++) jmax = max(jmax, s_pt[g].count);
+  for (int j = warp; j < jmax; j += blockDim.x >> 5)
+    for (int g = 0; g < G; g++) {
+      const DualPoint &pt = s_pt[g];
+      if (j >= pt.count) continue;
+      const double2 *w = a.W + (size_t)(pt.k0 + j * a.stride) * cells;
+      const double2 *qg = q + (size_t)g * cells;
+      double re = 0.0, im = 0.0;
+      for (int c = lane; c < cells; c += 32) {
+        const double2 x = __ldg(w + c), z = qg[c];
+        re = fma(x.x, z.x, fma(-x.y, z.y, re));
+        im = fma(x.x, z.y, fma(x.y, z.x, im));
       }
-      me.P[me.rec0 + rec] = make_double2(pr, pi);
-      rec++;
-    }
-    for (int m = 4; m >= 1; m--) {
-      const double cm = a.h / m;
-      const T2 *W = w32 + (size_t)buf * cells;
-      T2 *Wn = w32 + (size_t)(buf ^ 1) * cells;
-      if (live) {
-        T kr[kTailMax], ki[kTailMax];
-        T2 zb[kTailMax];
-#pragma unroll
-        for (int e = 0; e < kTailMax; e++) {
-          kr[e] = 0;
-          ki[e] = 0;
-          zb[e] = e < ne ? W[e * pstride + blk] : mk2<T>(0.0, 0.0);
-        }
-#pragma unroll
-        for (int e = 0; e < kTailMax; e++) { // X = C z, k = -i X
-          if (e >= ne) break;
-#pragma unroll
-          for (int f = 0; f < kTailMax; f++) {
-            if (!(s_mask[e] & (1u << f))) continue;
-            const T2 c = s_C[e * kTailMax + f], z = zb[f];
-            ki[e] = fma(-c.x, z.x, ki[e]);
-            ki[e] = fma(c.y, z.y, ki[e]);
-            kr[e] = fma(c.x, z.y, kr[e]);
-            kr[e] = fma(c.y, z.x, kr[e]);
-          }
-        }
-        const T2 *Wp = W + pp * nado; // this point's ADOs, position e at e * pstride
-#pragma unroll
-        for (int e = 0; e < kTailMax; e++) { // bath links of site levels r (row) and c (column)
-          if (e >= ne) break;
-          const int q = s_pos[e], r = q / NT, c = q - r * NT;
-          const T2 *We = Wp + e * pstride;
-          if (r >= 1 && r <= K)
-            for (int k = 0; k < Km; k++) {
-              const PmLink<T> L = links[((r - 1) + k * K) * nado + n];
-              const unsigned u = (unsigned)L.ud & 0xffffu, d = (unsigned)L.ud >> 16;
-              if (u != 0xffffu && c != r) {
-                const T2 z = We[u];
-                kr[e] = fma(-L.x, z.y, kr[e]);
-                ki[e] = fma(L.x, z.x, ki[e]);
-              }
-              if (d != 0xffffu) {
-                const T2 z = We[d];
-                const T cr = c == r ? -2 * L.by : -L.by, ci = c == r ? (T)0 : L.ay;
-                kr[e] = fma(cr, z.x, fma(-ci, z.y, kr[e]));
-                ki[e] = fma(cr, z.y, fma(ci, z.x, ki[e]));
-              }
-            }
-          if (c >= 1 && c <= K && c != r)
-            for (int k = 0; k < Km; k++) {
-              const PmLink<T> L = links[((c - 1) + k * K) * nado + n];
-              const unsigned u = (unsigned)L.ud & 0xffffu, d = (unsigned)L.ud >> 16;
-              if (u != 0xffffu) {
-                const T2 z = We[u];
-                kr[e] = fma(L.x, z.y, kr[e]);
-                ki[e] = fma(-L.x, z.x, ki[e]);
-              }
-              if (d != 0xffffu) {
-                const T2 z = We[d];
-                kr[e] = fma(-L.by, z.x, fma(L.ay, z.y, kr[e]));
-                ki[e] = fma(-L.by, z.y, fma(-L.ay, z.x, ki[e]));
-              }
-            }
-        }
-#pragma unroll
-        for (int e = 0; e < kTailMax; e++) { // FP64: damping + site-energy diagonal, Horner update
-          if (e >= ne) break;
-          const double gr = dmp.x, gi = dmp.y + s_gi[e];
-          const double2 wv = w64[e];
-          const double k_r = fma(gr, wv.x, fma(-gi, wv.y, (double)kr[e]));
-          const double k_i = fma(gr, wv.y, fma(gi, wv.x, (double)ki[e]));
-          const double2 r0v = rho[e * pstride + blk];
-          const double2 wn = make_double2(fma(cm, k_r, r0v.x), fma(cm, k_i, r0v.y));
-          w64[e] = wn;
-          Wn[e * pstride + blk] = mk2<T>(wn.x, wn.y);
-          if (m == 1) rho[e * pstride + blk] = wn;
-        }
+      for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
       }
-      buf ^= 1;
-      __syncthreads();
+      if (lane == 0) pt.P[j] = make_double2(re, im);
     }
-    t += a.dt;
-  }
 }
