@@ -1694,6 +1694,21 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       jobs.push_back(K.job);
     }
   if (jobs.empty()) return 0;
+  { // every index and pointer the slot kernel will follow, checked against its buffer
+    const double2 *s0 = snap, *s1 = snap + s.snap_cap;
+    auto in_snap = [&](const double2 *q) { return q >= s0 && q + snap_elems <= s1; };
+    const char *bad = nullptr;
+    for (const SlotJob &J : jobs) {
+      for (int k = 0; k < 4; k++)
+        if (J.wait[k] >= n) bad = "wait flag";
+      if (J.first < 0 || J.last < J.first || J.save_begin < 0 || J.save_end > (int)saves.size()) bad = "job range";
+      for (const SlotSpec &z : J.slot)
+        if (z.init == 2 && !in_snap(z.init_ptr)) bad = "initial snapshot";
+    }
+    for (const SlotSave &sv : saves)
+      if (sv.flag >= n || !in_snap(sv.dst)) bad = "save";
+    if (bad) { s_err = std::string("staged scan plan check failed: ") + bad; return HEOM_ERR_CUDA; }
+  }
   e = grow<SlotJob>(s.d_jobs, s.jobs_cap, jobs.size());
   if (e == cudaSuccess) e = grow<SlotSave>(s.d_saves, s.saves_cap, std::max<size_t>(saves.size(), 1));
   if (e != cudaSuccess) { s_err = "staged scan job tables: out of device memory"; return HEOM_ERR_NOMEM; }
