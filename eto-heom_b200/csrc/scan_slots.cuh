@@ -167,6 +167,48 @@ __device__ __forceinline__ void sl_stage(const PmShared &g, int n, int blk, unsi
   }
 }
 
+// The same stage for row R0 of the slot's block only (steps with a single live slot: the
+// block's rows are spread over four threads).  Per element the operations and their
+// order are those of sl_stage.
+template <typename T, int NT, int R0>
+__device__ __forceinline__ void sl_stage_row(const PmShared &g, int n, int blk, unsigned am,
+                                             const typename V2<T>::t *A, int sb0, unsigned sm0,
+                                             const typename V2<T>::t *S0, int sb1, unsigned sm1,
+                                             const typename V2<T>::t *S1, const typename V2<T>::t *__restrict__ W,
+                                             typename V2<T>::t *__restrict__ Wn, const double *__restrict__ Hdd,
+                                             double2 *__restrict__ rho, const PmLink<T> *__restrict__ links, int slot,
+                                             double2 dmp, double cm, bool last, double2 (&w64)[NT]) {
+  using T2 = typename V2<T>::t;
+  const int SP = g.SP, nado = g.nado, K = g.K, Km = g.Km;
+  T kr[NT], ki[NT];
+#pragma unroll
+  for (int e = 0; e < NT; e++) { kr[e] = 0; ki[e] = 0; }
+  if (am) pm_commutator<T, NT, 1, R0>(am, A, W, SP, blk, kr, ki);
+#pragma unroll 1
+  for (int k = 0; k < 2; k++) {
+    const int sb = k == 0 ? sb0 : sb1;
+    const unsigned sm = k == 0 ? sm0 : sm1;
+    if (sb >= 0 && sm) pm_commutator<T, NT, 1, R0>(sm, k == 0 ? S0 : S1, W, SP, sb * nado + n, kr, ki);
+  }
+  const T2 *Wc = W + slot * nado;
+  if (K >= 1) pm_links<T, NT, 1, R0, 1>(Wc, SP, nado, K, Km, n, links, kr, ki);
+  if (NT > 2 && K >= 2) pm_links<T, NT, 1, R0, (NT > 2 ? 2 : 1)>(Wc, SP, nado, K, Km, n, links, kr, ki);
+  if (NT > 3 && K >= 3) pm_links<T, NT, 1, R0, (NT > 3 ? 3 : 1)>(Wc, SP, nado, K, Km, n, links, kr, ki);
+#pragma unroll
+  for (int c = 0; c < NT; c++) {
+    const int q = R0 * NT + c;
+    const double gr = dmp.x, gi = dmp.y - Hdd[q];
+    const double2 wv = w64[c];
+    const double k_r = fma(gr, wv.x, fma(-gi, wv.y, (double)kr[c]));
+    const double k_i = fma(gr, wv.y, fma(gi, wv.x, (double)ki[c]));
+    const double2 r0v = rho[q * SP + blk];
+    const double2 wn = make_double2(fma(cm, k_r, r0v.x), fma(cm, k_i, r0v.y));
+    w64[c] = wn;
+    Wn[q * SP + blk] = mk2<T>(wn.x, wn.y);
+    if (last) rho[q * SP + blk] = wn;
+  }
+}
+
 // One Horner stage of the reduced tail: positions tpos[0..ne) of the slot's block.
 template <typename T, int NT>
 __device__ __forceinline__ void sl_stage_tail(const PmShared &g, int n, int blk, int slot, int ne,
@@ -426,6 +468,7 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
     int sv = J.save_begin;
     int next_save = sv < J.save_end ? a.saves[sv].step : 0x7fffffff;
     int buf = 0;
+    bool fieldfree = false; // the operators in shared memory were built for a step with no field on
     float t = s_t0;
     __syncthreads(); // field tables complete
     for (int i = first; i <= last; i++) {
@@ -459,7 +502,14 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
       for (int r = 0; r < 4; r++)
         rec[r] = J.rec[r].q >= 0 && i >= J.rec[r].first && i < J.rec[r].last && t >= J.rec[r].tau3 &&
                  i % a.stride == 0;
-      if (tid < 32) {
+      // With no pulse on and no record due, the operators and masks of the last field-free
+      // step still hold: skip warp 0's rebuild and its barrier (uniform across the CTA).
+      bool anyon = false;
+#pragma unroll
+      for (int w = 0; w < 6; w++) anyon = anyon || on[w];
+      const bool rebuild = anyon || rec[0] || rec[1] || rec[2] || rec[3] || !fieldfree;
+      fieldfree = !anyon;
+      if (rebuild && tid < 32) {
         // warp 0: the slots' operators, the pulse-2/3 operators of both field sets, their
         // nonzero masks, and the traces of the recorders' slots (one element per lane)
         const int q = tid;
@@ -536,7 +586,7 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
             }
           }
       }
-      __syncthreads();
+      if (rebuild) __syncthreads();
       if (tid == 0)
 #pragma unroll
         for (int r = 0; r < 4; r++)
@@ -546,6 +596,53 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
           }
 #pragma unroll
       for (int r = 0; r < 4; r++) rcn[r] += rec[r];
+      // a single live full-block slot: its rows are spread over all threads
+      int nlive = 0, ss = 0;
+#pragma unroll
+      for (int z = 0; z < 4; z++)
+        if (i >= J.slot[z].wake && i < J.slot[z].stop) { nlive++; ss = z; }
+      if (nlive == 1 && J.mode == 0 && NT * nado <= bs) {
+        const int r = tid / nado, n2 = tid - r * nado;
+        const bool ok = r < NT;
+        const SlotSpec &sp = J.slot[ss];
+        const int blk2 = ss * nado + (ok ? n2 : 0);
+        const unsigned am2 = s_mask[ss];
+        const int f2 = sp.fset;
+        const bool s0 = sp.src[0] >= 0 && on[3 * f2 + sp.srcq[0]];
+        const bool s1 = sp.src[1] >= 0 && on[3 * f2 + sp.srcq[1]];
+        const int b0 = s0 ? sp.src[0] : -1, b1 = s1 ? sp.src[1] : -1;
+        const unsigned k0 = s0 ? s_mask[4 + 2 * f2 + sp.srcq[0] - 1] : 0u;
+        const unsigned k1 = s1 ? s_mask[4 + 2 * f2 + sp.srcq[1] - 1] : 0u;
+        const T2 *Q0 = Aall + (4 + 2 * f2 + (s0 ? sp.srcq[0] - 1 : 0)) * NN;
+        const T2 *Q1 = Aall + (4 + 2 * f2 + (s1 ? sp.srcq[1] - 1 : 0)) * NN;
+        const double2 dmp2 = ok ? sdamp[n2] : make_double2(0.0, 0.0);
+        double2 wr[NT];
+#pragma unroll
+        for (int c = 0; c < NT; c++) wr[c] = ok ? rho[(r * NT + c) * SP + blk2] : make_double2(0.0, 0.0);
+        for (int m = 4; m >= 1; m--) {
+          const double cm = a.h / m;
+          const T2 *W = w32 + (size_t)buf * EP;
+          T2 *Wn = w32 + (size_t)(buf ^ 1) * EP;
+          if (ok) {
+            if (r == 0)
+              sl_stage_row<T, NT, 0>(gsh, n2, blk2, am2, Aall + ss * NN, b0, k0, Q0, b1, k1, Q1, W, Wn, Hdd, rho,
+                                     links, ss, dmp2, cm, m == 1, wr);
+            else if (r == 1)
+              sl_stage_row<T, NT, (NT > 1 ? 1 : 0)>(gsh, n2, blk2, am2, Aall + ss * NN, b0, k0, Q0, b1, k1, Q1, W,
+                                                    Wn, Hdd, rho, links, ss, dmp2, cm, m == 1, wr);
+            else if (r == 2)
+              sl_stage_row<T, NT, (NT > 2 ? 2 : 0)>(gsh, n2, blk2, am2, Aall + ss * NN, b0, k0, Q0, b1, k1, Q1, W,
+                                                    Wn, Hdd, rho, links, ss, dmp2, cm, m == 1, wr);
+            else
+              sl_stage_row<T, NT, (NT > 3 ? 3 : 0)>(gsh, n2, blk2, am2, Aall + ss * NN, b0, k0, Q0, b1, k1, Q1, W,
+                                                    Wn, Hdd, rho, links, ss, dmp2, cm, m == 1, wr);
+          }
+          buf ^= 1;
+          __syncthreads();
+        }
+        t += a.dt;
+        continue;
+      }
       const bool live = sl >= 0 && i >= my.wake && i < my.stop;
       const int blk = live ? sl * nado + n : 0;
       const unsigned am = live ? s_mask[sl] : 0u;
