@@ -41,6 +41,7 @@
 #include <cstdlib>
 #include <complex>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -935,6 +936,7 @@ static void tail_table(const std::vector<double> &sys, int N, std::vector<double
 }
 
 static void dual_operator(ScanState &s, const std::vector<double> &sys, const std::vector<double> &tab);
+static void jump_operator(ScanState &s, const std::vector<double> &sys);
 
 int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
   if (!s.supported) return 0;
@@ -948,6 +950,7 @@ int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
     if (e != cudaSuccess) { s_err = std::string("tail table upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
     if (s.tail_n > 0) dual_operator(s, sys, tab);
   }
+  if (s.staged) jump_operator(s, sys);
   { // the kernels' test for a stationary |0><0| (off-diagonal H in row and column 0)
     const double *Hoff = sys.data() + s.N;
     bool z = true;
@@ -1316,48 +1319,61 @@ template <class T> static cudaError_t grow(void *&ptr, size_t &cap, size_t want)
   return e;
 }
 
-// Dual tails.  The pulse-free operator on the reduced cells (cell = e * n_ado + n:
-// position e of the tail table, ADO n in the kernels' order), in FP64, as the tail
-// arithmetic defines it: -i C z (the restricted commutator), the bath links of the
-// cell's site row r and site column c, and (damping + i (damping' - (H_rr - H_cc))) z.
-// Kept transposed (CSR of L^T) with the readout vector x3 (Tr X3 . on ADO 0) as w_0.
-static void dual_operator(ScanState &s, const std::vector<double> &sys, const std::vector<double> &tab) {
-  const int ne = (int)tab[0], nado = s.n_ado, K = s.K, Km = s.K_m, N = s.N, NN = N * N, cells = ne * nado;
+// The pulse-free HEOM operator (no field on) restricted to a set of element positions
+// closed under the off-diagonal H, in FP64: for cell = e * n_ado + n (position pos[e],
+// ADO n in the kernels' order) emit(cell, cell', value) for every entry L[cell][cell'],
+// as the propagation kernels define the operator: (damping + i (damping' - (H_rr - H_cc)))
+// on the diagonal, -i C (C: the commutator with the off-diagonal H restricted to the
+// positions), and the bath links of the cell's site row r and site column c.
+template <class Emit>
+static void pulse_free_terms(const ScanState &s, const std::vector<double> &sys, const std::vector<int> &pos,
+                             Emit emit) {
+  const int ne = (int)pos.size(), nado = s.n_ado, K = s.K, Km = s.K_m, N = s.N;
   const TableLayout tl(nado, s.M, Km);
   const PmLinkHost *L = (const PmLinkHost *)(s.h_tables.data() + tl.plink);
   const double *dmp = (const double *)(s.h_tables.data() + tl.pdamp);
-  const double *Hd = sys.data(), *X3 = sys.data() + N + 2 * NN + 6 * NN;
-  const double *C = tab.data() + 1 + kTailMax;
-  std::vector<std::vector<std::pair<int, std::complex<double>>>> lt(cells); // lt[c'] : (c, L[c][c'])
-  s.dual_diag.assign(2 * (size_t)cells, 0.0);
-  auto add = [&](int c, int c2, std::complex<double> v) { lt[c2].push_back({c, v}); };
+  const double *Hd = sys.data(), *Hoff = sys.data() + N;
   const std::complex<double> I(0.0, 1.0);
   for (int e = 0; e < ne; e++) {
-    const int q = (int)tab[1 + e], r = q / N, c = q - r * N;
+    const int r = pos[e] / N, c = pos[e] % N;
     for (int n = 0; n < nado; n++) {
       const int cell = e * nado + n;
+      emit(cell, cell, std::complex<double>(dmp[2 * n], dmp[2 * n + 1] - (Hd[r] - Hd[c])));
       for (int f = 0; f < ne; f++) {
-        const std::complex<double> cf(C[2 * (e * kTailMax + f)], C[2 * (e * kTailMax + f) + 1]);
-        if (cf != 0.0) add(cell, f * nado + n, -I * cf);
+        const int l = pos[f] / N, c2 = pos[f] % N;
+        double cr = 0.0, ci = 0.0;
+        if (c2 == c) { cr += Hoff[2 * (r * N + l)]; ci += Hoff[2 * (r * N + l) + 1]; }   // (H w)[r][c]
+        if (l == r) { cr -= Hoff[2 * (c2 * N + c)]; ci -= Hoff[2 * (c2 * N + c) + 1]; } // (w H)[r][c]
+        if (cr != 0.0 || ci != 0.0) emit(cell, f * nado + n, -I * std::complex<double>(cr, ci));
       }
       if (r >= 1 && r <= K)
         for (int k = 0; k < Km; k++) {
-          const PmLinkHost &l = L[(size_t)((r - 1) + k * K) * nado + n];
-          const unsigned u = (unsigned)l.ud & 0xffffu, d = (unsigned)l.ud >> 16;
-          if (u != 0xffffu && c != r) add(cell, e * nado + (int)u, I * l.x);
-          if (d != 0xffffu) add(cell, e * nado + (int)d, std::complex<double>(c == r ? -2 * l.by : -l.by, c == r ? 0.0 : l.ay));
+          const PmLinkHost &lk = L[(size_t)((r - 1) + k * K) * nado + n];
+          const unsigned u = (unsigned)lk.ud & 0xffffu, d = (unsigned)lk.ud >> 16;
+          if (u != 0xffffu && c != r) emit(cell, e * nado + (int)u, I * lk.x);
+          if (d != 0xffffu)
+            emit(cell, e * nado + (int)d, std::complex<double>(c == r ? -2 * lk.by : -lk.by, c == r ? 0.0 : lk.ay));
         }
       if (c >= 1 && c <= K && c != r)
         for (int k = 0; k < Km; k++) {
-          const PmLinkHost &l = L[(size_t)((c - 1) + k * K) * nado + n];
-          const unsigned u = (unsigned)l.ud & 0xffffu, d = (unsigned)l.ud >> 16;
-          if (u != 0xffffu) add(cell, e * nado + (int)u, -I * l.x);
-          if (d != 0xffffu) add(cell, e * nado + (int)d, std::complex<double>(-l.by, -l.ay));
+          const PmLinkHost &lk = L[(size_t)((c - 1) + k * K) * nado + n];
+          const unsigned u = (unsigned)lk.ud & 0xffffu, d = (unsigned)lk.ud >> 16;
+          if (u != 0xffffu) emit(cell, e * nado + (int)u, -I * lk.x);
+          if (d != 0xffffu) emit(cell, e * nado + (int)d, std::complex<double>(-lk.by, -lk.ay));
         }
-      s.dual_diag[2 * cell] = dmp[2 * n];
-      s.dual_diag[2 * cell + 1] = dmp[2 * n + 1] - (Hd[r] - Hd[c]);
     }
   }
+}
+
+// Dual tails: L^T on the reduced cells (CSR, the diagonal included) and the readout
+// vector x3 (Tr X3 . on ADO 0) as w_0.
+static void dual_operator(ScanState &s, const std::vector<double> &sys, const std::vector<double> &tab) {
+  const int ne = (int)tab[0], nado = s.n_ado, N = s.N, NN = N * N, cells = ne * nado;
+  const double *X3 = sys.data() + N + 2 * NN + 6 * NN;
+  std::vector<int> pos(ne);
+  for (int e = 0; e < ne; e++) pos[e] = (int)tab[1 + e];
+  std::vector<std::vector<std::pair<int, std::complex<double>>>> lt(cells); // lt[c'] : (c, L[c][c'])
+  pulse_free_terms(s, sys, pos, [&](int c, int c2, std::complex<double> v) { lt[c2].push_back({c, v}); });
   s.dual_start.assign(cells + 1, 0);
   s.dual_idx.clear();
   s.dual_coef.clear();
@@ -1372,15 +1388,148 @@ static void dual_operator(ScanState &s, const std::vector<double> &sys, const st
   s.dual_start[cells] = (int)s.dual_idx.size();
   s.h_W.assign(2 * (size_t)cells, 0.0); // w_0 = x3: P = sum_e X3[c][r] Q[e][ADO 0]
   for (int e = 0; e < ne; e++) {
-    const int q = (int)tab[1 + e], r = q / N, c = q - r * N;
+    const int r = pos[e] / N, c = pos[e] % N;
     s.h_W[2 * ((size_t)e * nado + s.ado0)] = X3[2 * (c * N + r)];
     s.h_W[2 * ((size_t)e * nado + s.ado0) + 1] = X3[2 * (c * N + r) + 1];
   }
   s.W_rows = 1;
   s.W_dev_rows = 0;
-  s.dual_pos.assign(ne, 0);
-  for (int e = 0; e < ne; e++) s.dual_pos[e] = (int)tab[1 + e];
+  s.dual_pos = pos;
   s.dual_pos_dirty = true;
+}
+
+// Jumps: the pulse-free step map T0 = sum_{j<=4} (h L0)^j / j! is block-diagonal over the
+// connected components of the element positions under the off-diagonal H (the bath acts
+// within a position).  Per sample the host builds L0 of each block densely; the device
+// forms T0 (Horner, FP64) and its squares T0^(2^j) on demand (jump_powers).
+static void jump_operator(ScanState &s, const std::vector<double> &sys) {
+  const int N = s.N, NN = N * N, nado = s.n_ado;
+  const double *Hoff = sys.data() + N;
+  std::vector<int> comp(NN);
+  for (int q = 0; q < NN; q++) comp[q] = q;
+  std::function<int(int)> find = [&](int q) { return comp[q] == q ? q : comp[q] = find(comp[q]); };
+  auto nz = [&](int r, int c) { return Hoff[2 * (r * N + c)] != 0.0 || Hoff[2 * (r * N + c) + 1] != 0.0; };
+  for (int r = 0; r < N; r++)
+    for (int c = 0; c < N; c++)
+      for (int l = 0; l < N; l++) {
+        if (l != r && nz(r, l)) comp[find(r * N + c)] = find(l * N + c);
+        if (l != c && nz(l, c)) comp[find(r * N + c)] = find(r * N + l);
+      }
+  std::vector<std::vector<int>> blocks;
+  std::vector<int> bid(NN, -1);
+  for (int q = 0; q < NN; q++) {
+    const int root = find(q);
+    if (bid[root] < 0) { bid[root] = (int)blocks.size(); blocks.emplace_back(); }
+    blocks[bid[root]].push_back(q);
+  }
+  const int nb = (int)blocks.size();
+  s.jtab.assign(1 + 3 * nb + NN, 0);
+  s.jtab[0] = nb;
+  long long off = 0;
+  int pf = 0;
+  std::vector<long long> boff(nb);
+  for (int b = 0; b < nb; b++) {
+    const long long d = (long long)blocks[b].size() * nado;
+    s.jtab[1 + b] = (int)blocks[b].size();
+    s.jtab[1 + nb + b] = pf;
+    s.jtab[1 + 2 * nb + b] = (int)off;
+    boff[b] = off;
+    for (int q : blocks[b]) s.jtab[1 + 3 * nb + pf++] = q;
+    off += d * d;
+  }
+  s.jpow_elems = off;
+  s.h_jL.assign(2 * (size_t)off, 0.0);
+  for (int b = 0; b < nb; b++) {
+    const long long d = (long long)blocks[b].size() * nado;
+    double *Lb = s.h_jL.data() + 2 * boff[b];
+    pulse_free_terms(s, sys, blocks[b], [&](int c, int c2, std::complex<double> v) {
+      Lb[2 * (c * d + c2)] += v.real();
+      Lb[2 * (c * d + c2) + 1] += v.imag();
+    });
+  }
+  s.jblocks = blocks.size();
+  s.jdims.resize(nb);
+  for (int b = 0; b < nb; b++) s.jdims[b] = (int)blocks[b].size() * nado;
+  s.jpow_n = 0;    // powers must be recomputed for this sample
+  s.jL_dirty = true;
+}
+
+// C = ident * I + alpha * A B for square d x d complex FP64 matrices (row-major): the
+// Horner steps of T0 = T4(h L0) and the squarings T0^(2^(j+1)) = (T0^(2^j))^2.
+__global__ void jump_gemm(int d, double alpha, int ident, const double2 *__restrict__ A,
+                          const double2 *__restrict__ B, double2 *__restrict__ C) {
+  __shared__ double2 As[16][17], Bs[16][17];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int row = blockIdx.y * 16 + ty, col = blockIdx.x * 16 + tx;
+  double re = 0.0, im = 0.0;
+  for (int k0 = 0; k0 < d; k0 += 16) {
+    As[ty][tx] = (row < d && k0 + tx < d) ? A[(size_t)row * d + k0 + tx] : make_double2(0.0, 0.0);
+    Bs[ty][tx] = (k0 + ty < d && col < d) ? B[(size_t)(k0 + ty) * d + col] : make_double2(0.0, 0.0);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      const double2 x = As[ty][k], y = Bs[k][tx];
+      re = fma(x.x, y.x, fma(-x.y, y.y, re));
+      im = fma(x.x, y.y, fma(x.y, y.x, im));
+    }
+    __syncthreads();
+  }
+  if (row < d && col < d)
+    C[(size_t)row * d + col] = make_double2((ident && row == col ? 1.0 : 0.0) + alpha * re, alpha * im);
+}
+
+// Powers T0^(2^j), j < need, of every jump block on the device (cached per sample).
+static int jump_powers(ScanState &s, int need, cudaStream_t st) {
+  cudaError_t e = cudaSuccess;
+  const size_t pe = (size_t)s.jpow_elems;
+  if (s.jL_dirty) {
+    if (s.d_jtab) cudaFree(s.d_jtab);
+    if (s.d_jL) cudaFree(s.d_jL);
+    if (s.d_jtmp) cudaFree(s.d_jtmp);
+    s.d_jtab = s.d_jL = s.d_jtmp = nullptr;
+    e = cudaMalloc(&s.d_jtab, sizeof(int) * s.jtab.size());
+    if (e == cudaSuccess) e = cudaMalloc(&s.d_jL, sizeof(double2) * pe);
+    if (e == cudaSuccess) e = cudaMalloc(&s.d_jtmp, 2 * sizeof(double2) * pe);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s.d_jtab, s.jtab.data(), sizeof(int) * s.jtab.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_jL, s.h_jL.data(), sizeof(double2) * pe, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    s.jpow_n = 0;
+    s.jL_dirty = false;
+  }
+  if (e == cudaSuccess && need > s.jpow_cap) {
+    if (s.d_jpow) cudaFree(s.d_jpow);
+    s.d_jpow = nullptr;
+    s.jpow_cap = 0;
+    s.jpow_n = 0;
+    e = cudaMalloc(&s.d_jpow, sizeof(double2) * pe * need);
+    if (e == cudaSuccess) s.jpow_cap = need;
+  }
+  if (e != cudaSuccess) { s_err = std::string("jump tables: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  double2 *L = (double2 *)s.d_jL, *P = (double2 *)s.d_jpow, *X0 = (double2 *)s.d_jtmp, *X1 = X0 + pe;
+  const int nb = s.jtab[0];
+  auto gemm = [&](int d, double alpha, int ident, const double2 *A, const double2 *B, double2 *C) {
+    const dim3 g((d + 15) / 16, (d + 15) / 16), t(16, 16);
+    jump_gemm<<<g, t, 0, st>>>(d, alpha, ident, A, B, C);
+  };
+  for (int j = s.jpow_n; j < need; j++)
+    for (int b = 0; b < nb; b++) {
+      const int d = s.jdims[b];
+      const size_t o = (size_t)s.jtab[1 + 2 * nb + b];
+      if (j == 0) { // Horner: X = I; X = I + (h/m) L X, m = 4..1
+        gemm(d, 0.0, 1, L + o, L + o, X0 + o);
+        gemm(d, s.h / 4, 1, L + o, X0 + o, X1 + o);
+        gemm(d, s.h / 3, 1, L + o, X1 + o, X0 + o);
+        gemm(d, s.h / 2, 1, L + o, X0 + o, X1 + o);
+        gemm(d, s.h, 1, L + o, X1 + o, P + o);
+      } else {
+        gemm(d, 1.0, 0, P + (j - 1) * pe + o, P + (j - 1) * pe + o, P + j * pe + o);
+      }
+    }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) { s_err = std::string("jump powers: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  s.jpow_n = std::max(s.jpow_n, need);
+  return 0;
 }
 
 // Extend the dual vectors to `rows` (w_{k+1} = T4(h L^T) w_k in Horner form, FP64) and
@@ -1390,14 +1539,13 @@ static int dual_rows(ScanState &s, int rows, cudaStream_t st) {
   if (s.W_rows < rows) {
     s.h_W.resize(2 * (size_t)cells * rows);
     std::vector<double> u(2 * (size_t)cells), lu(2 * (size_t)cells);
-    const double *D = s.dual_diag.data(), *Cf = s.dual_coef.data();
+    const double *Cf = s.dual_coef.data();
     for (int k = s.W_rows; k < rows; k++) {
       const double *w = s.h_W.data() + 2 * (size_t)cells * (k - 1);
       std::copy(w, w + 2 * (size_t)cells, u.begin());
       for (int m = 4; m >= 1; m--) { // u = w + (h/m) L^T u (complex arithmetic written out)
         for (int c2 = 0; c2 < cells; c2++) {
-          double ar = D[2 * c2] * u[2 * c2] - D[2 * c2 + 1] * u[2 * c2 + 1];
-          double ai = D[2 * c2] * u[2 * c2 + 1] + D[2 * c2 + 1] * u[2 * c2];
+          double ar = 0.0, ai = 0.0;
           for (int j = s.dual_start[c2]; j < s.dual_start[c2 + 1]; j++) {
             const double *z = u.data() + 2 * (size_t)s.dual_idx[j];
             ar += Cf[2 * j] * z[0] - Cf[2 * j + 1] * z[1];
@@ -1462,11 +1610,14 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   // state at its window end
   std::vector<long long> snap_of(n, -1);
   for (size_t k = 0; k < regular.size(); k++) snap_of[regular[k]] = 3 * (long long)k;
-  cudaError_t e = grow<double2>(s.d_snap, s.snap_cap, std::max<size_t>(3 * regular.size(), 1) * snap_elems);
-  if (e == cudaSuccess) e = grow<int>(s.d_flags, s.flags_cap, (size_t)n + 1); // + the error word
+  // plus one jump base (D2 at the end of stage 1) per (tau1, tau2) group; flags: one per
+  // point, the error word, one per group
+  cudaError_t e = grow<double2>(s.d_snap, s.snap_cap, std::max<size_t>(4 * regular.size(), 1) * snap_elems);
+  if (e == cudaSuccess) e = grow<int>(s.d_flags, s.flags_cap, (size_t)n + 1 + regular.size());
   if (e != cudaSuccess) { s_err = "staged scan snapshots: out of device memory"; return HEOM_ERR_NOMEM; }
   double2 *snap = (double2 *)s.d_snap;
   auto state = [&](int i, int which) { return snap + (size_t)(snap_of[i] + which) * snap_elems; };
+  auto gsnap = [&](size_t g) { return snap + (3 * regular.size() + g) * snap_elems; };
   double2 *P = (double2 *)d_P;
   auto count_recs = [&](int i, int from, int to) {
     return records_before(s, pl[i], to) - records_before(s, pl[i], from);
@@ -1493,7 +1644,9 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     if (pts[a].tau2 != pts[b].tau2) return pts[a].tau2 < pts[b].tau2;
     return pl[a].s2 < pl[b].s2;
   });
-  struct Group { int lead, first, last, rlast; std::vector<int> members; }; // rlast: R's last step
+  // rlast: R's last step; d2stop: D2's (the jump base step when members jump); jumped:
+  // two-component members reached by jumps from the base
+  struct Group { int lead, first, last, rlast, d2stop; std::vector<int> members, jumped; };
   std::vector<Group> groups;
   for (size_t g0 = 0; g0 < order.size();) {
     size_t g1 = g0;
@@ -1516,11 +1669,55 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
         if (!two[i]) G.rlast = std::max(G.rlast, std::max(pl[i].s2, G.first));
       G.rlast = std::min(G.rlast, G.last);
     }
+    // Jumps: once pulses 1 and 2 are off (step f), R and D2 evolve under the pulse-free map
+    // T0 until pulse 3; two-component members whose window starts after the base step b
+    // (f, or the latest four-component member's window start) get D2 there by T0^(s2 - b).
+    G.d2stop = G.last;
+    {
+      const PtPlan &q = pl[G.lead];
+      int b = std::max(q.cnt[0] > 0 ? q.lo[0] + q.cnt[0] : 0, q.cnt[1] > 0 ? q.lo[1] + q.cnt[1] : 0);
+      b = std::max(b, G.first);
+      for (int i : G.members)
+        if (!two[i]) b = std::max(b, std::max(pl[i].s2, G.first));
+      for (int i : G.members)
+        if (two[i] && pl[i].s2 > b) G.jumped.push_back(i);
+      if (!G.jumped.empty()) G.d2stop = b;
+    }
     groups.push_back(G);
     g0 = g1;
   }
   std::sort(groups.begin(), groups.end(),
-            [](const Group &a, const Group &b) { return a.last - a.first > b.last - b.first; });
+            [](const Group &a, const Group &b) { return a.d2stop - a.first > b.d2stop - b.first; });
+  std::vector<Keyed> qj; // jump jobs: per group a chain through its jumped members in window order
+  int jmax = 0;          // longest jump (steps)
+  for (size_t g = 0; g < groups.size(); g++) {
+    const Group &G = groups[g];
+    int base_step = G.d2stop, base_flag = n + 1 + (int)g;
+    const double2 *base = gsnap(g);
+    for (int i : G.jumped) { // members are in window order
+      Keyed K;
+      SlotJob &J = K.job;
+      J = SlotJob{};
+      J.mode = 2;
+      J.first = base_step;
+      J.last = pl[i].s2;
+      J.wait[0] = base_flag;
+      J.wait[1] = J.wait[2] = J.wait[3] = -1;
+      J.wait_val = 1;
+      set_taus(J, 0, pts[i]);
+      set_taus(J, 1, pts[i]);
+      for (int h = 0; h < 4; h++) { J.slot[h] = slot_off(); J.rec[h] = rec_off(); }
+      J.slot[0].init = 2;
+      J.slot[0].init_ptr = base;
+      K.saves.push_back(SlotSave{J.last, 0, -1, i, 1, 0, state(i, 1)});
+      K.key = base_step;
+      jmax = std::max(jmax, J.last - J.first);
+      qj.push_back(std::move(K));
+      base_step = pl[i].s2;
+      base_flag = i;
+      base = state(i, 1);
+    }
+  }
   const size_t solo = std::min<size_t>(groups.size(), (size_t)std::max(0, kSoloGroups));
   for (size_t g = 0; g < groups.size(); g += g < solo ? 1 : 2) {
     const size_t ng = g < solo ? 1 : 2; // the longest groups alone: they set the critical path
@@ -1538,16 +1735,19 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       const PtPlan &q = pl[G.lead];
       set_taus(J, h, pts[G.lead]);
       J.first = std::min(J.first, G.first);
-      J.last = std::max(J.last, G.last);
-      J.slot[2 * h] = slot_mk(1, h, q.wR, G.rlast, 1, nullptr);
-      J.slot[2 * h + 1] = slot_mk(3, h, q.wD2, G.last, 0, nullptr);
+      J.last = std::max(J.last, G.d2stop);
+      J.slot[2 * h] = slot_mk(1, h, q.wR, std::min(G.rlast, G.d2stop), 1, nullptr);
+      J.slot[2 * h + 1] = slot_mk(3, h, q.wD2, G.d2stop, 0, nullptr);
       J.slot[2 * h + 1].src[0] = 2 * h;
       J.slot[2 * h + 1].srcq[0] = 1;
       for (int i : G.members) {
+        if (std::find(G.jumped.begin(), G.jumped.end(), i) != G.jumped.end()) continue;
         const int st2 = std::max(pl[i].s2, G.first);
         if (!two[i]) K.saves.push_back(SlotSave{st2, 2 * h, -1, -1, 0, 0, state(i, 0)});
         K.saves.push_back(SlotSave{st2, 2 * h + 1, -1, i, 1, 0, state(i, 1)});
       }
+      if (!G.jumped.empty()) // the jump base
+        K.saves.push_back(SlotSave{G.d2stop, 2 * h + 1, -1, n + 1 + (int)(g + h), 1, 0, gsnap(g + h)});
     }
     std::stable_sort(K.saves.begin(), K.saves.end(), [](const SlotSave &a, const SlotSave &b) { return a.step < b.step; });
     for (SlotSave &sv : K.saves) sv.step = std::max(sv.step, J.first);
@@ -1683,6 +1883,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   }
   // queue: stage 1 (longest first), then stages 2 and 3 in the order their inputs become
   // ready (window start for stage 2, window end for stage 3)
+  for (Keyed &K : qj) q23.push_back(std::move(K));
   std::stable_sort(q23.begin(), q23.end(), [](const Keyed &a, const Keyed &b) { return a.key < b.key; });
   std::vector<SlotJob> jobs;
   std::vector<SlotSave> saves;
@@ -1694,19 +1895,32 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       jobs.push_back(K.job);
     }
   if (jobs.empty()) return 0;
+  if (jmax > 0) {
+    int need = 0;
+    while ((jmax >> need) != 0) need++;
+    const int rc = jump_powers(s, need, st);
+    if (rc) return rc;
+  }
   { // every index and pointer the slot kernel will follow, checked against its buffer
+    const long long nflags = (long long)n + 1 + (long long)groups.size();
     const double2 *s0 = snap, *s1 = snap + s.snap_cap;
     auto in_snap = [&](const double2 *q) { return q >= s0 && q + snap_elems <= s1; };
     const char *bad = nullptr;
     for (const SlotJob &J : jobs) {
       for (int k = 0; k < 4; k++)
-        if (J.wait[k] >= n) bad = "wait flag";
+        if (J.wait[k] >= nflags) bad = "wait flag";
       if (J.first < 0 || J.last < J.first || J.save_begin < 0 || J.save_end > (int)saves.size()) bad = "job range";
       for (const SlotSpec &z : J.slot)
         if (z.init == 2 && !in_snap(z.init_ptr)) bad = "initial snapshot";
+      if (J.mode == 2) {
+        if (J.save_end != J.save_begin + 1 || !in_snap(J.slot[0].init_ptr)) bad = "jump";
+        if ((long long)(J.last - J.first) >> s.jpow_n != 0 && J.last > J.first) bad = "jump length";
+        if (!s.d_jpow || !s.d_jtab) bad = "jump tables";
+      }
     }
-    for (const SlotSave &sv : saves)
-      if (sv.flag >= n || !in_snap(sv.dst)) bad = "save";
+    for (const SlotSave &sv : saves) {
+      if (sv.flag >= nflags || !in_snap(sv.dst)) bad = "save";
+    }
     if (bad) { s_err = std::string("staged scan plan check failed: ") + bad; return HEOM_ERR_CUDA; }
   }
   e = grow<SlotJob>(s.d_jobs, s.jobs_cap, jobs.size());
@@ -1716,7 +1930,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   if (e == cudaSuccess && !saves.empty())
     e = cudaMemcpyAsync(s.d_saves, saves.data(), sizeof(SlotSave) * saves.size(), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.d_counter, 0, sizeof(int), st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(s.d_flags, 0, sizeof(int) * ((size_t)n + 1), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.d_flags, 0, sizeof(int) * ((size_t)n + 1 + groups.size()), st);
   if (e != cudaSuccess) { s_err = std::string("staged scan upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
   SlotArgs a{};
   a.N = s.N;
@@ -1741,6 +1955,10 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   a.err = (int *)s.d_flags + n;
   a.wait_ns = 30ull * 1000 * 1000 * 1000; // far above any legitimate wait
   a.tail = s.tail_n > 0 ? (const double *)s.d_tail : nullptr;
+  a.jtab = (const int *)s.d_jtab;
+  a.jpow = (const double2 *)s.d_jpow;
+  a.jpow_stride = s.jpow_elems;
+  a.jpow_n = s.jpow_n;
   const int grid = std::max(1, std::min(a.n_jobs, s.sl_grid));
   slot_kernel(s.precision)<<<grid, s.sl_threads, s.sl_smem, st>>>(a);
   e = cudaGetLastError();
@@ -1781,6 +1999,9 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       da.pos = (const int *)s.d_dualpos;
       da.W = (const double2 *)s.d_W;
       da.pts = (const DualPoint *)s.d_tailpts;
+      da.NN = s.N * s.N;
+      da.W_rows = s.W_dev_rows;
+      da.err = (int *)s.d_flags + n;
       const size_t smem = sizeof(double2) * (size_t)kDualG * s.tail_n * s.n_ado;
       e = cudaFuncSetAttribute(scan_tail_dual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e == cudaSuccess) {
@@ -1809,7 +2030,8 @@ int staged_status(ScanState &s, cudaStream_t st) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) { s_err = std::string("staged scan status: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
   s.err_pending = nullptr;
-  if (err) { s_err = "staged scan: a stage waited too long for its inputs"; return HEOM_ERR_TIMEOUT; }
+  if (err == 1) { s_err = "staged scan: a stage waited too long for its inputs"; return HEOM_ERR_TIMEOUT; }
+  if (err) { s_err = "staged scan: internal check " + std::to_string(err) + " failed"; return HEOM_ERR_CUDA; }
   return 0;
 }
 
@@ -1928,6 +2150,10 @@ void scan_release(ScanState &s) {
   if (s.d_tailpts) cudaFree(s.d_tailpts);
   if (s.d_W) cudaFree(s.d_W);
   if (s.d_dualpos) cudaFree(s.d_dualpos);
+  if (s.d_jtab) cudaFree(s.d_jtab);
+  if (s.d_jL) cudaFree(s.d_jL);
+  if (s.d_jpow) cudaFree(s.d_jpow);
+  if (s.d_jtmp) cudaFree(s.d_jtmp);
   if (s.d_jobs) cudaFree(s.d_jobs);
   if (s.d_saves) cudaFree(s.d_saves);
   if (s.d_tables) cudaFree(s.d_tables);

@@ -63,11 +63,20 @@ struct ScanState {
   // diagonal, w_k rows on the host and the device, the reduced positions
   std::vector<unsigned char> h_tables;
   std::vector<int> dual_start, dual_idx, dual_pos;
-  std::vector<double> dual_coef, dual_diag, h_W;
+  std::vector<double> dual_coef, h_W;
   int W_rows = 0, W_dev_rows = 0;
   bool dual_pos_dirty = false;
   void *d_W = nullptr, *d_dualpos = nullptr;
   size_t W_cap = 0;
+  // jumps over pulse-free intervals: position blocks (jtab: count, positions per block,
+  // first position, matrix offset, positions), dense L0 blocks, powers T0^(2^j) on device
+  std::vector<int> jtab, jdims;
+  std::vector<double> h_jL;
+  long long jpow_elems = 0;
+  size_t jblocks = 0;
+  int jpow_n = 0, jpow_cap = 0;
+  bool jL_dirty = false;
+  void *d_jtab = nullptr, *d_jL = nullptr, *d_jpow = nullptr, *d_jtmp = nullptr;
   std::vector<heom_scan_point> rb_pts; // points / offsets read back for heom_run_scan_device
   std::vector<long long> rb_off;
   long long staged_launches = 0;

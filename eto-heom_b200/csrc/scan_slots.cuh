@@ -93,6 +93,10 @@ struct SlotArgs {
   int *err;              // set to 1 when a dependency wait gives up
   unsigned long long wait_ns;
   const double *tail;    // [n][pos x kTailMax][C: kTailMax x kTailMax complex], see tail_table
+  const int *jtab;       // jump blocks: count, positions per block, first position, offset, positions
+  const double2 *jpow;   // T0^(2^j) of every block, jpow_stride elements per power
+  long long jpow_stride;
+  int jpow_n;            // powers available
 };
 
 constexpr int kTailMax = 8;
@@ -294,6 +298,69 @@ __device__ __forceinline__ void sl_stage_tail(const PmShared &g, int n, int blk,
   }
 }
 
+// A jump job (mode 2): the state snapshot slot[0].init_ptr at step `first` carried to step
+// `last` with no field on, as T0^(last - first) applied through the powers T0^(2^j) of each
+// position block (dense FP64 block mat-vecs, one warp per row); the result goes to the
+// job's first save, whose flag is then raised.  sbuf: 2 x n_ado * NN doubles2 of scratch.
+template <int NT>
+__device__ void sl_jump(const SlotArgs &a, const SlotJob &J, double2 *sbuf, int tid, int bs) {
+  constexpr int NN = NT * NT;
+  const int nado = a.n_ado, cells = NN * nado;
+  double2 *x = sbuf, *y = sbuf + cells;
+  for (int e = tid; e < cells; e += bs) x[e] = __ldcg(J.slot[0].init_ptr + e);
+  __syncthreads();
+  const int nb = a.jtab[0];
+  const int *np = a.jtab + 1, *pfirst = a.jtab + 1 + nb, *moff = a.jtab + 1 + 2 * nb, *plist = a.jtab + 1 + 3 * nb;
+  const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
+  const int delta = J.last - J.first;
+  for (int j = 0; (delta >> j) != 0; j++) {
+    if (!((delta >> j) & 1)) continue;
+    if (j >= a.jpow_n) { // powers not prepared: give up (checked error, no access)
+      if (tid == 0) atomicMax(a.err, 3);
+      break;
+    }
+    const double2 *Pj = a.jpow + (size_t)j * a.jpow_stride;
+    for (int b = 0; b < nb; b++) {
+      const int d = np[b] * nado;
+      const int *pos = plist + pfirst[b];
+      const double2 *Pb = Pj + moff[b];
+      if ((long long)moff[b] + (long long)d * d > a.jpow_stride || pfirst[b] + np[b] > NN) {
+        if (tid == 0) atomicMax(a.err, 4);
+        continue;
+      }
+      for (int row = warp; row < d; row += nw) {
+        const double2 *Pr = Pb + (size_t)row * d;
+        double re = 0.0, im = 0.0;
+        for (int col = lane; col < d; col += 32) {
+          const double2 m = __ldg(Pr + col);
+          const int f = col / nado;
+          const double2 z = x[pos[f] * nado + (col - f * nado)];
+          re = fma(m.x, z.x, fma(-m.y, z.y, re));
+          im = fma(m.x, z.y, fma(m.y, z.x, im));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          re += __shfl_xor_sync(0xffffffffu, re, o);
+          im += __shfl_xor_sync(0xffffffffu, im, o);
+        }
+        if (lane == 0) {
+          const int er = row / nado;
+          y[pos[er] * nado + (row - er * nado)] = make_double2(re, im);
+        }
+      }
+    }
+    __syncthreads();
+    double2 *t = x;
+    x = y;
+    y = t;
+  }
+  const SlotSave &sv = a.saves[J.save_begin];
+  for (int e = tid; e < cells; e += bs) __stcg(sv.dst + e, x[e]);
+  __threadfence();
+  __syncthreads();
+  if (tid == 0 && sv.flag >= 0) atomicMax(a.flags + sv.flag, sv.fval);
+}
+
 template <typename T, int NT, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
   using T2 = typename V2<T>::t;
@@ -410,6 +477,10 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
         for (int k = J.save_begin; k < J.save_end; k++)
           if (a.saves[k].flag >= 0) atomicMax(a.flags + a.saves[k].flag, a.saves[k].fval);
       }
+      continue;
+    }
+    if (J.mode == 2) { // jump: pulse-free steps [first, last) as powers of T0
+      sl_jump<NT>(a, J, rho, tid, bs);
       continue;
     }
     // Pulse windows of both field sets (absolute step indices), and the float time at
@@ -592,7 +663,10 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
         for (int r = 0; r < 4; r++)
           if (rec[r]) {
             const int k = J.rec[r].rec0 + rcn[r];
-            J.rec[r].P[k] = make_double2(s_tr[2 * r].x - s_tr[2 * r + 1].x, s_tr[2 * r].y - s_tr[2 * r + 1].y);
+            if (rcn[r] < J.rec[r].nrec)
+              J.rec[r].P[k] = make_double2(s_tr[2 * r].x - s_tr[2 * r + 1].x, s_tr[2 * r].y - s_tr[2 * r + 1].y);
+            else
+              atomicMax(a.err, 2); // more records than planned: skipped
           }
 #pragma unroll
       for (int r = 0; r < 4; r++) rcn[r] += rec[r];
@@ -703,10 +777,11 @@ struct DualPoint {
 };
 
 struct DualArgs {
-  int ne, nado, stride, n_pts;
+  int ne, nado, stride, n_pts, NN, W_rows;
   const int *pos;        // the reduced positions (r * N + c)
   const double2 *W;      // w_k, [k][cell], cell = e * nado + n
   const DualPoint *pts;
+  int *err;              // set when a check fails (the access is skipped)
 };
 
 __global__ void __launch_bounds__(kDualThreads) scan_tail_dual(DualArgs a) {
@@ -719,7 +794,9 @@ __global__ void __launch_bounds__(kDualThreads) scan_tail_dual(DualArgs a) {
   __syncthreads();
   for (int t = tid; t < G * cells; t += blockDim.x) {
     const int g = t / cells, c = t - g * cells, e = c / a.nado, n = c - e * a.nado;
-    q[t] = __ldcg(s_pt[g].q + (size_t)a.pos[e] * a.nado + n);
+    const int ps = a.pos[e];
+    if (ps < 0 || ps >= a.NN) { atomicMax(a.err, 5); q[t] = make_double2(0.0, 0.0); continue; }
+    q[t] = __ldcg(s_pt[g].q + (size_t)ps * a.nado + n);
   }
   __syncthreads();
   int jmax = 0;
@@ -728,6 +805,10 @@ __global__ void __launch_bounds__(kDualThreads) scan_tail_dual(DualArgs a) {
     for (int g = 0; g < G; g++) {
       const DualPoint &pt = s_pt[g];
       if (j >= pt.count) continue;
+      if (pt.k0 + j * a.stride >= a.W_rows) {
+        if (lane == 0) atomicMax(a.err, 6);
+        continue;
+      }
       const double2 *w = a.W + (size_t)(pt.k0 + j * a.stride) * cells;
       const double2 *qg = q + (size_t)g * cells;
       double re = 0.0, im = 0.0;
