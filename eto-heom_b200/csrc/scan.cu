@@ -1921,6 +1921,22 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     for (const SlotSave &sv : saves) {
       if (sv.flag >= nflags || !in_snap(sv.dst)) bad = "save";
     }
+    if (!qj.empty()) { // block table: the positions once each, every block inside a power
+      const int nb = s.jtab.empty() ? 0 : s.jtab[0], NN = s.N * s.N;
+      std::vector<char> seen(NN, 0);
+      int pos_total = 0;
+      for (int b = 0; b < nb && !bad; b++) {
+        const long long d = (long long)s.jtab[1 + b] * s.n_ado;
+        if (s.jtab[1 + nb + b] != pos_total || s.jtab[1 + 2 * nb + b] + d * d > (long long)s.jpow_elems) bad = "jump block";
+        for (int k = 0; k < s.jtab[1 + b] && !bad; k++) {
+          const int q = s.jtab[1 + 3 * nb + pos_total + k];
+          if (q < 0 || q >= NN || seen[q]) bad = "jump positions";
+          else seen[q] = 1;
+        }
+        pos_total += s.jtab[1 + b];
+      }
+      if (pos_total != NN) bad = "jump positions";
+    }
     if (bad) { s_err = std::string("staged scan plan check failed: ") + bad; return HEOM_ERR_CUDA; }
   }
   e = grow<SlotJob>(s.d_jobs, s.jobs_cap, jobs.size());

@@ -298,19 +298,92 @@ __device__ __forceinline__ void sl_stage_tail(const PmShared &g, int n, int blk,
   }
 }
 
+// One position block's rows of y = P x, both block-ordered: a warp takes RW rows at a time
+// and lane l their columns l + 32 u (u < U, 32 U >= d), so each lane has RW * U
+// independent loads of P in flight before its first FMA; the block's x stays in registers.
+template <int U, int RW>
+__device__ __forceinline__ void jump_rows(const double2 *__restrict__ P, const double2 *xb, double2 *yb, int d,
+                                          int lane, int warp, int nw) {
+  double2 xv[U];
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    const int c = lane + 32 * u;
+    xv[u] = c < d ? xb[c] : make_double2(0.0, 0.0);
+  }
+  for (int r0 = warp * RW; r0 < d; r0 += nw * RW) {
+    double2 m[RW][U];
+#pragma unroll
+    for (int k = 0; k < RW; k++)
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int c = lane + 32 * u;
+        m[k][u] = (r0 + k < d && c < d) ? __ldg(P + (size_t)(r0 + k) * d + c) : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+    for (int k = 0; k < RW; k++) {
+      double re = 0.0, im = 0.0;
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        re = fma(m[k][u].x, xv[u].x, fma(-m[k][u].y, xv[u].y, re));
+        im = fma(m[k][u].x, xv[u].y, fma(m[k][u].y, xv[u].x, im));
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
+      }
+      if (lane == 0 && r0 + k < d) yb[r0 + k] = make_double2(re, im);
+    }
+  }
+}
+
+// Rows of a block wider than the register tiles: one row per warp, 8 loads per lane in flight.
+__device__ __forceinline__ void jump_rows_wide(const double2 *__restrict__ P, const double2 *xb, double2 *yb, int d,
+                                               int lane, int warp, int nw) {
+  for (int r = warp; r < d; r += nw) {
+    const double2 *Pr = P + (size_t)r * d;
+    double re = 0.0, im = 0.0;
+    for (int c0 = 0; c0 < d; c0 += 256) {
+      double2 m[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int c = c0 + lane + 32 * u;
+        m[u] = c < d ? __ldg(Pr + c) : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int c = c0 + lane + 32 * u;
+        const double2 z = c < d ? xb[c] : make_double2(0.0, 0.0);
+        re = fma(m[u].x, z.x, fma(-m[u].y, z.y, re));
+        im = fma(m[u].x, z.y, fma(m[u].y, z.x, im));
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      re += __shfl_xor_sync(0xffffffffu, re, o);
+      im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    if (lane == 0) yb[r] = make_double2(re, im);
+  }
+}
+
 // A jump job (mode 2): the state snapshot slot[0].init_ptr at step `first` carried to step
 // `last` with no field on, as T0^(last - first) applied through the powers T0^(2^j) of each
-// position block (dense FP64 block mat-vecs, one warp per row); the result goes to the
-// job's first save, whose flag is then raised.  sbuf: 2 x n_ado * NN doubles2 of scratch.
+// position block (dense FP64 block mat-vecs).  The state is held in block order (the
+// positions of jtab's list, each with its n_ado ADOs) from the gather to the save.
+// sbuf: 2 x n_ado * NN doubles2 of scratch.
 template <int NT>
 __device__ void sl_jump(const SlotArgs &a, const SlotJob &J, double2 *sbuf, int tid, int bs) {
   constexpr int NN = NT * NT;
   const int nado = a.n_ado, cells = NN * nado;
   double2 *x = sbuf, *y = sbuf + cells;
-  for (int e = tid; e < cells; e += bs) x[e] = __ldcg(J.slot[0].init_ptr + e);
-  __syncthreads();
   const int nb = a.jtab[0];
   const int *np = a.jtab + 1, *pfirst = a.jtab + 1 + nb, *moff = a.jtab + 1 + 2 * nb, *plist = a.jtab + 1 + 3 * nb;
+  for (int e = tid; e < cells; e += bs) {
+    const int f = e / nado;
+    x[e] = __ldcg(J.slot[0].init_ptr + plist[f] * nado + (e - f * nado));
+  }
+  __syncthreads();
   const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
   const int delta = J.last - J.first;
   for (int j = 0; (delta >> j) != 0; j++) {
@@ -321,33 +394,20 @@ __device__ void sl_jump(const SlotArgs &a, const SlotJob &J, double2 *sbuf, int 
     }
     const double2 *Pj = a.jpow + (size_t)j * a.jpow_stride;
     for (int b = 0; b < nb; b++) {
-      const int d = np[b] * nado;
-      const int *pos = plist + pfirst[b];
-      const double2 *Pb = Pj + moff[b];
+      const int d = np[b] * nado, o = pfirst[b] * nado;
       if ((long long)moff[b] + (long long)d * d > a.jpow_stride || pfirst[b] + np[b] > NN) {
         if (tid == 0) atomicMax(a.err, 4);
         continue;
       }
-      for (int row = warp; row < d; row += nw) {
-        const double2 *Pr = Pb + (size_t)row * d;
-        double re = 0.0, im = 0.0;
-        for (int col = lane; col < d; col += 32) {
-          const double2 m = __ldg(Pr + col);
-          const int f = col / nado;
-          const double2 z = x[pos[f] * nado + (col - f * nado)];
-          re = fma(m.x, z.x, fma(-m.y, z.y, re));
-          im = fma(m.x, z.y, fma(m.y, z.x, im));
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          re += __shfl_xor_sync(0xffffffffu, re, o);
-          im += __shfl_xor_sync(0xffffffffu, im, o);
-        }
-        if (lane == 0) {
-          const int er = row / nado;
-          y[pos[er] * nado + (row - er * nado)] = make_double2(re, im);
-        }
-      }
+      const double2 *Pb = Pj + moff[b];
+      if (d <= 96)
+        jump_rows<3, 4>(Pb, x + o, y + o, d, lane, warp, nw);
+      else if (d <= 160)
+        jump_rows<5, 3>(Pb, x + o, y + o, d, lane, warp, nw);
+      else if (d <= 288)
+        jump_rows<9, 2>(Pb, x + o, y + o, d, lane, warp, nw);
+      else
+        jump_rows_wide(Pb, x + o, y + o, d, lane, warp, nw);
     }
     __syncthreads();
     double2 *t = x;
@@ -355,7 +415,10 @@ __device__ void sl_jump(const SlotArgs &a, const SlotJob &J, double2 *sbuf, int 
     y = t;
   }
   const SlotSave &sv = a.saves[J.save_begin];
-  for (int e = tid; e < cells; e += bs) __stcg(sv.dst + e, x[e]);
+  for (int e = tid; e < cells; e += bs) {
+    const int f = e / nado;
+    __stcg(sv.dst + plist[f] * nado + (e - f * nado), x[e]);
+  }
   __threadfence();
   __syncthreads();
   if (tid == 0 && sv.flag >= 0) atomicMax(a.flags + sv.flag, sv.fval);
