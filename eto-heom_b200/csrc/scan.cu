@@ -1587,6 +1587,51 @@ static int dual_rows(ScanState &s, int rows, cudaStream_t st) {
   return 0;
 }
 
+// Slot-steps of a slot job that the kernel jumps over instead of propagating: the pulse-free
+// gaps of scan_slots' step loop, found by the same rule (no pulse of either field set on,
+// no save, slot wake or stop, or record inside; at least kGapMin steps).  Accounting only.
+static long long gap_steps(const ScanState &s, const TimeGrid &g, const SlotJob &J, const std::vector<SlotSave> &saves,
+                           int jpow) {
+  if (J.mode != 0 || jpow <= 0) return 0;
+  int lo[6], cn[6];
+  const float *t = g.t.data();
+  for (int w = 0; w < 6; w++) { // the kernel's windows: steps in [0, last) with |t - tau| <= 2 taup
+    const double tw = 2 * s.taup[w % 3], tq = J.tau[w / 3][w % 3];
+    const int a = TimeGrid::first_true(J.last, [&](int i) { return (double)t[i] - tq >= -tw; });
+    const int b = TimeGrid::first_true(J.last, [&](int i) { return (double)t[i] - tq > tw; });
+    lo[w] = a < b ? a : 0;
+    cn[w] = a < b ? b - a : 0;
+  }
+  long long skipped = 0;
+  int sv = J.save_begin;
+  for (int i = J.first; i < J.last;) {
+    while (sv < J.save_end && saves[sv].step <= i) sv++;
+    int ge = std::min(J.last, sv < J.save_end ? saves[sv].step : 0x7fffffff);
+    ge = std::min(ge, i + (1 << std::min(jpow, 30)) - 1);
+    for (int w = 0; w < 6; w++)
+      if (cn[w] > 0) {
+        if ((unsigned)(i - lo[w]) < (unsigned)cn[w]) ge = i;
+        else if (lo[w] > i) ge = std::min(ge, lo[w]);
+      }
+    for (int z = 0; z < 4; z++) {
+      if (J.slot[z].wake > i) ge = std::min(ge, J.slot[z].wake);
+      if (J.slot[z].stop > i) ge = std::min(ge, J.slot[z].stop);
+      if (J.rec[z].q >= 0) {
+        if (i >= J.rec[z].first && i < J.rec[z].last) ge = i;
+        else if (J.rec[z].first > i) ge = std::min(ge, J.rec[z].first);
+      }
+    }
+    if (ge - i >= kGapMin) {
+      for (int z = 0; z < 4; z++)
+        if (J.slot[z].wake <= i && i < J.slot[z].stop) skipped += ge - i;
+      i = ge;
+    } else {
+      i++;
+    }
+  }
+  return skipped;
+}
+
 int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, const long long *offsets,
                cudaStream_t st) {
   const int NN = s.N * s.N;
@@ -1895,10 +1940,15 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       jobs.push_back(K.job);
     }
   if (jobs.empty()) return 0;
-  if (jmax > 0) {
-    int need = 0;
-    while ((jmax >> need) != 0) need++;
-    const int rc = jump_powers(s, need, st);
+  // powers for the jump jobs and for the pulse-free gaps inside slot jobs (up to a job's
+  // length); without a block table no gap is jumped
+  int jlong = jmax;
+  for (const SlotJob &J : jobs)
+    if (J.mode == 0) jlong = std::max(jlong, J.last - J.first);
+  int jpow_use = 0;
+  if (jlong > 0 && !s.jtab.empty()) {
+    while ((jlong >> jpow_use) != 0) jpow_use++;
+    const int rc = jump_powers(s, jpow_use, st);
     if (rc) return rc;
   }
   { // every index and pointer the slot kernel will follow, checked against its buffer
@@ -1914,14 +1964,14 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
         if (z.init == 2 && !in_snap(z.init_ptr)) bad = "initial snapshot";
       if (J.mode == 2) {
         if (J.save_end != J.save_begin + 1 || !in_snap(J.slot[0].init_ptr)) bad = "jump";
-        if ((long long)(J.last - J.first) >> s.jpow_n != 0 && J.last > J.first) bad = "jump length";
+        if ((long long)(J.last - J.first) >> jpow_use != 0 && J.last > J.first) bad = "jump length";
         if (!s.d_jpow || !s.d_jtab) bad = "jump tables";
       }
     }
     for (const SlotSave &sv : saves) {
       if (sv.flag >= nflags || !in_snap(sv.dst)) bad = "save";
     }
-    if (!qj.empty()) { // block table: the positions once each, every block inside a power
+    if (jpow_use > 0) { // block table: the positions once each, every block inside a power
       const int nb = s.jtab.empty() ? 0 : s.jtab[0], NN = s.N * s.N;
       std::vector<char> seen(NN, 0);
       int pos_total = 0;
@@ -1974,7 +2024,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   a.jtab = (const int *)s.d_jtab;
   a.jpow = (const double2 *)s.d_jpow;
   a.jpow_stride = s.jpow_elems;
-  a.jpow_n = s.jpow_n;
+  a.jpow_n = jpow_use; // prepared for this sample by jump_powers above
   const int grid = std::max(1, std::min(a.n_jobs, s.sl_grid));
   slot_kernel(s.precision)<<<grid, s.sl_threads, s.sl_smem, st>>>(a);
   e = cudaGetLastError();
@@ -2032,7 +2082,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   for (const SlotJob &J : jobs) { // propagated component-steps (a reduced step counts its share)
     long long w = 0;
     for (const SlotSpec &z : J.slot) w += std::max(0, std::min(z.stop, J.last) - std::max(z.wake, J.first));
-    s.last_work += J.mode == 1 ? w * s.tail_n / (s.N * s.N) : w;
+    s.last_work += J.mode == 1 ? w * s.tail_n / (s.N * s.N) : w - gap_steps(s, tgrid, J, saves, jpow_use);
   }
   return 0;
 }

@@ -100,6 +100,7 @@ struct SlotArgs {
 };
 
 constexpr int kTailMax = 8;
+constexpr int kGapMin = 8; // shortest pulse-free gap a slot job jumps over (steps)
 // Reduced-tail table (doubles): [0] = n positions (0: none), [1..kTailMax] = positions
 // r*N + c, then C (kTailMax x kTailMax complex, row-major): X_e = sum_e' C[e][e'] w_e' is
 // the commutator [H_off, w] restricted to the positions.
@@ -367,25 +368,15 @@ __device__ __forceinline__ void jump_rows_wide(const double2 *__restrict__ P, co
   }
 }
 
-// A jump job (mode 2): the state snapshot slot[0].init_ptr at step `first` carried to step
-// `last` with no field on, as T0^(last - first) applied through the powers T0^(2^j) of each
-// position block (dense FP64 block mat-vecs).  The state is held in block order (the
-// positions of jtab's list, each with its n_ado ADOs) from the gather to the save.
-// sbuf: 2 x n_ado * NN doubles2 of scratch.
-template <int NT>
-__device__ void sl_jump(const SlotArgs &a, const SlotJob &J, double2 *sbuf, int tid, int bs) {
-  constexpr int NN = NT * NT;
-  const int nado = a.n_ado, cells = NN * nado;
-  double2 *x = sbuf, *y = sbuf + cells;
+// T0^delta applied to the block-ordered state x (the positions of jtab's list, each with
+// its n_ado ADOs; y: scratch of the same size) as one dense block mat-vec per set bit of
+// delta, through the powers T0^(2^j).  Every thread of the CTA calls it; returns the
+// buffer that holds the result.
+__device__ double2 *jump_apply(const SlotArgs &a, double2 *x, double2 *y, int delta, int NN, int tid, int bs) {
+  const int nado = a.n_ado;
   const int nb = a.jtab[0];
-  const int *np = a.jtab + 1, *pfirst = a.jtab + 1 + nb, *moff = a.jtab + 1 + 2 * nb, *plist = a.jtab + 1 + 3 * nb;
-  for (int e = tid; e < cells; e += bs) {
-    const int f = e / nado;
-    x[e] = __ldcg(J.slot[0].init_ptr + plist[f] * nado + (e - f * nado));
-  }
-  __syncthreads();
+  const int *np = a.jtab + 1, *pfirst = a.jtab + 1 + nb, *moff = a.jtab + 1 + 2 * nb;
   const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
-  const int delta = J.last - J.first;
   for (int j = 0; (delta >> j) != 0; j++) {
     if (!((delta >> j) & 1)) continue;
     if (j >= a.jpow_n) { // powers not prepared: give up (checked error, no access)
@@ -414,6 +405,24 @@ __device__ void sl_jump(const SlotArgs &a, const SlotJob &J, double2 *sbuf, int 
     x = y;
     y = t;
   }
+  return x;
+}
+
+// A jump job (mode 2): the state snapshot slot[0].init_ptr at step `first` carried to step
+// `last` with no field on, as T0^(last - first); the result goes to the job's first save,
+// whose flag is then raised.  sbuf: 2 x n_ado * NN doubles2 of scratch.
+template <int NT>
+__device__ void sl_jump(const SlotArgs &a, const SlotJob &J, double2 *sbuf, int tid, int bs) {
+  constexpr int NN = NT * NT;
+  const int nado = a.n_ado, cells = NN * nado;
+  const int *plist = a.jtab + 1 + 3 * a.jtab[0];
+  double2 *x = sbuf;
+  for (int e = tid; e < cells; e += bs) {
+    const int f = e / nado;
+    x[e] = __ldcg(J.slot[0].init_ptr + plist[f] * nado + (e - f * nado));
+  }
+  __syncthreads();
+  x = jump_apply(a, x, sbuf + cells, J.last - J.first, NN, tid, bs);
   const SlotSave &sv = a.saves[J.save_begin];
   for (int e = tid; e < cells; e += bs) {
     const int f = e / nado;
@@ -628,6 +637,57 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
             if (a.saves[k].flag >= 0) atomicMax(a.flags + a.saves[k].flag, a.saves[k].fval);
       }
       if (i == last) break;
+      // A pulse-free gap: no pulse of either field set on, and no save, slot wake or stop,
+      // or record inside.  Every live slot then evolves under the pulse-free map alone, so
+      // the slots jump over the gap as T0^(gap) (FP64 block powers) instead of stepping.
+      if (J.mode == 0 && a.jpow_n > 0) {
+        int ge = min(last, next_save);
+        ge = min(ge, i + (1 << min(a.jpow_n, 30)) - 1);
+#pragma unroll
+        for (int w = 0; w < 6; w++)
+          if (cn[w] > 0) {
+            if ((unsigned)(i - lo[w]) < (unsigned)cn[w]) ge = i;
+            else if (lo[w] > i) ge = min(ge, lo[w]);
+          }
+#pragma unroll
+        for (int z = 0; z < 4; z++) {
+          if (J.slot[z].wake > i) ge = min(ge, J.slot[z].wake);
+          if (J.slot[z].stop > i) ge = min(ge, J.slot[z].stop);
+          if (J.rec[z].q >= 0) {
+            if (i >= J.rec[z].first && i < J.rec[z].last) ge = i;
+            else if (J.rec[z].first > i) ge = min(ge, J.rec[z].first);
+          }
+        }
+        if (ge - i >= kGapMin) {
+          const int cells = NN * nado;
+          const int *plist = a.jtab + 1 + 3 * a.jtab[0];
+          double2 *gx = (double2 *)w32, *gy = gx + cells; // the FP32 copies are rebuilt below
+          for (int z = 0; z < 4; z++) {
+            if (!(J.slot[z].wake <= i && i < J.slot[z].stop)) continue;
+            for (int e = tid; e < cells; e += bs) {
+              const int f = e / nado;
+              gx[e] = rho[plist[f] * SP + z * nado + (e - f * nado)];
+            }
+            __syncthreads();
+            const double2 *r = jump_apply(a, gx, gy, ge - i, NN, tid, bs);
+            for (int e = tid; e < cells; e += bs) {
+              const int f = e / nado;
+              rho[plist[f] * SP + z * nado + (e - f * nado)] = r[e];
+            }
+            __syncthreads();
+          }
+          for (size_t e = tid; e < EP; e += bs) {
+            const double2 v = rho[e];
+            w32[e] = mk2<T>(v.x, v.y);
+            w32[EP + e] = mk2<T>(v.x, v.y);
+          }
+          __syncthreads();
+          for (int k = i; k < ge; k++) t += a.dt;
+          fieldfree = false;
+          i = ge - 1;
+          continue;
+        }
+      }
       bool on[6];
 #pragma unroll
       for (int w = 0; w < 6; w++) on[w] = (unsigned)(i - lo[w]) < (unsigned)cn[w];
