@@ -104,6 +104,8 @@ def lib() -> ctypes.CDLL:
         "heom_plan_describe": (I, [P, ctypes.c_char_p, I]),
         "heom_plan_launch_count": (ctypes.c_longlong, [P]),
         "heom_plan_scan_work": (ctypes.c_longlong, [P]),
+        "heom_plan_sync": (I, [P]),
+        "heom_plan_inject_wait_fault": (I, [P, ctypes.c_ulonglong, I]),
         "heom_plan_destroy": (None, [P]),
         "heom_measure_fma_peak": (I, [I, I, D]),
         "heom_run_scan_noalloc": (I, [P, I, P, I, P, P, P]),
@@ -315,9 +317,19 @@ class Plan:
         return ScanResult(P[:tot], off, cnt), grad
 
     def run_scan_device(self, d_pts: int, n: int, d_P: int, d_offsets: int) -> None:
-        """Device-pointer form (e.g. torch tensors' data_ptr()); asynchronous on the plan's stream."""
+        """Device-pointer form (e.g. torch tensors' data_ptr()); asynchronous on the plan's
+        stream.  Errors found on the device are reported by sync() (or the next scan call)."""
         _check(lib().heom_run_scan_device(self._h, ctypes.c_void_p(d_pts), n, ctypes.c_void_p(d_P),
                                           ctypes.c_void_p(d_offsets)))
+
+    def sync(self) -> None:
+        """Wait for the plan's queued work; raises HeomError with its deferred status."""
+        _check(lib().heom_plan_sync(self._h))
+
+    def inject_wait_fault(self, wait_ns: int, unmet: bool = True) -> None:
+        """Test hook: the next staged scan waits at most wait_ns per dependency and, with
+        unmet, one job waits for a flag that no producer sets (heom_plan_inject_wait_fault)."""
+        _check(lib().heom_plan_inject_wait_fault(self._h, int(wait_ns), 1 if unmet else 0))
 
 
 def fma_peak_tflops(device: int = 0, fp64: bool = False) -> float:

@@ -567,6 +567,27 @@ int heom_run_scan_device(heom_plan *pl, const heom_scan_point *d_pts, int n, dou
   return HEOM_OK;
 }
 
+int heom_plan_sync(heom_plan *pl) {
+  if (!pl) return fail(HEOM_ERR_ARG, "null plan");
+  CK(cudaSetDevice(pl->device));
+  if (pl->prob.dynamics || !pl->scan.supported) {
+    CK(cudaStreamSynchronize(pl->stream));
+    return HEOM_OK;
+  }
+  int rc = heom_dev::scan_sync(pl->scan, pl->stream);
+  if (rc) return fail(rc, heom_dev::scan_last_error());
+  return HEOM_OK;
+}
+
+int heom_plan_inject_wait_fault(heom_plan *pl, unsigned long long wait_ns, int unmet) {
+  if (!pl) return fail(HEOM_ERR_ARG, "null plan");
+  if (!pl->scan.supported || !pl->scan.staged) return fail(HEOM_ERR_UNSUPPORTED, "the plan does not run staged scans");
+  if (wait_ns == 0 || wait_ns > 60ull * 1000 * 1000 * 1000) return fail(HEOM_ERR_ARG, "wait limit outside (0, 60 s]");
+  pl->scan.inject_wait_ns = wait_ns;
+  pl->scan.inject_unmet = unmet != 0;
+  return HEOM_OK;
+}
+
 long long heom_plan_scan_work(const heom_plan *pl) {
   if (!pl) return fail(HEOM_ERR_ARG, "null plan");
   return pl->scan.staged ? pl->scan.last_work : 0;

@@ -1989,6 +1989,15 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     }
     if (bad) { s_err = std::string("staged scan plan check failed: ") + bad; return HEOM_ERR_CUDA; }
   }
+  const unsigned long long wait_ns = s.inject_wait_ns ? s.inject_wait_ns : 30ull * 1000 * 1000 * 1000;
+  if (s.inject_unmet) // test hook: the first consumer waits for a flag value no producer sets
+    for (SlotJob &J : jobs)
+      if (J.wait[0] >= 0 || J.wait[1] >= 0 || J.wait[2] >= 0 || J.wait[3] >= 0) {
+        J.wait_val = 0x7fffffff;
+        break;
+      }
+  s.inject_wait_ns = 0;
+  s.inject_unmet = false;
   e = grow<SlotJob>(s.d_jobs, s.jobs_cap, jobs.size());
   if (e == cudaSuccess) e = grow<SlotSave>(s.d_saves, s.saves_cap, std::max<size_t>(saves.size(), 1));
   if (e != cudaSuccess) { s_err = "staged scan job tables: out of device memory"; return HEOM_ERR_NOMEM; }
@@ -2019,7 +2028,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   a.n_jobs = (int)jobs.size();
   a.flags = (int *)s.d_flags;
   a.err = (int *)s.d_flags + n;
-  a.wait_ns = 30ull * 1000 * 1000 * 1000; // far above any legitimate wait
+  a.wait_ns = wait_ns; // by default far above any legitimate wait
   a.tail = s.tail_n > 0 ? (const double *)s.d_tail : nullptr;
   a.jtab = (const int *)s.d_jtab;
   a.jpow = (const double2 *)s.d_jpow;
@@ -2099,6 +2108,12 @@ int staged_status(ScanState &s, cudaStream_t st) {
   if (err == 1) { s_err = "staged scan: a stage waited too long for its inputs"; return HEOM_ERR_TIMEOUT; }
   if (err) { s_err = "staged scan: internal check " + std::to_string(err) + " failed"; return HEOM_ERR_CUDA; }
   return 0;
+}
+
+int scan_sync(ScanState &s, cudaStream_t st) {
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) { s_err = std::string("scan: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  return s.staged ? staged_status(s, st) : 0;
 }
 
 int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_points, bool tune, cudaStream_t st,

@@ -53,6 +53,9 @@ struct ScanState {
   void *d_jobs = nullptr, *d_saves = nullptr, *d_flags = nullptr;
   size_t jobs_cap = 0, saves_cap = 0, flags_cap = 0;
   int *err_pending = nullptr;    // error word of a run not yet checked
+  // test hook (heom_plan_inject_wait_fault): the next staged run only
+  unsigned long long inject_wait_ns = 0; // dependency wait limit (0: the default 30 s)
+  bool inject_unmet = false;     // one consumer job waits for a flag value never set
   long long last_work = 0;       // component-steps propagated by the last staged run
   std::vector<float> t_grid;     // float time of each step (t_start + dt accumulated)
   void *d_tail = nullptr;        // reduced-tail table of the current sample
@@ -101,6 +104,9 @@ int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, co
                   long long total, cudaStream_t st);
 int scan_run_device(ScanState &s, const heom_scan_point *d_pts, int n, double *d_P, const long long *d_offsets,
                     cudaStream_t st);
+// Waits for the stream and returns the status of the last staged run (HEOM_ERR_TIMEOUT
+// when a dependency wait gave up, HEOM_ERR_CUDA when a device-side check failed).
+int scan_sync(ScanState &s, cudaStream_t st);
 void scan_release(ScanState &s);
 std::string scan_describe(const ScanState &s);
 const char *scan_last_error();

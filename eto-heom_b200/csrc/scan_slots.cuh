@@ -371,16 +371,21 @@ __device__ __forceinline__ void jump_rows_wide(const double2 *__restrict__ P, co
 // T0^delta applied to the block-ordered state x (the positions of jtab's list, each with
 // its n_ado ADOs; y: scratch of the same size) as one dense block mat-vec per set bit of
 // delta, through the powers T0^(2^j).  Every thread of the CTA calls it; returns the
-// buffer that holds the result.
+// buffer that holds the result.  A failed check (powers not prepared, a block outside a
+// power) skips the access, sets the error word and fills the result with NaN, so that
+// every output depending on it reads NaN.  The checks read only values that are the same
+// for every thread, so all threads take the same branch.
 __device__ double2 *jump_apply(const SlotArgs &a, double2 *x, double2 *y, int delta, int NN, int tid, int bs) {
   const int nado = a.n_ado;
   const int nb = a.jtab[0];
   const int *np = a.jtab + 1, *pfirst = a.jtab + 1 + nb, *moff = a.jtab + 1 + 2 * nb;
   const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
+  bool bad = false;
   for (int j = 0; (delta >> j) != 0; j++) {
     if (!((delta >> j) & 1)) continue;
     if (j >= a.jpow_n) { // powers not prepared: give up (checked error, no access)
       if (tid == 0) atomicMax(a.err, 3);
+      bad = true;
       break;
     }
     const double2 *Pj = a.jpow + (size_t)j * a.jpow_stride;
@@ -388,6 +393,7 @@ __device__ double2 *jump_apply(const SlotArgs &a, double2 *x, double2 *y, int de
       const int d = np[b] * nado, o = pfirst[b] * nado;
       if ((long long)moff[b] + (long long)d * d > a.jpow_stride || pfirst[b] + np[b] > NN) {
         if (tid == 0) atomicMax(a.err, 4);
+        bad = true;
         continue;
       }
       const double2 *Pb = Pj + moff[b];
@@ -404,6 +410,11 @@ __device__ double2 *jump_apply(const SlotArgs &a, double2 *x, double2 *y, int de
     double2 *t = x;
     x = y;
     y = t;
+  }
+  if (bad) {
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    for (int e = tid; e < NN * nado; e += bs) x[e] = make_double2(nan, nan);
+    __syncthreads();
   }
   return x;
 }
@@ -540,10 +551,16 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
       s_ok = ok;
     }
     __syncthreads();
-    if (!s_ok) { // give up: NaN outputs, release dependants, report
+    if (!s_ok) { // give up: NaN outputs (first records, whole snapshots), release dependants, report
+      const double nan = __longlong_as_double(0x7ff8000000000000LL);
+      for (int k = J.save_begin; k < J.save_end; k++) {
+        double2 *dst = a.saves[k].dst;
+        for (size_t e = tid; e < (size_t)NN * nado; e += bs) __stcg(dst + e, make_double2(nan, nan));
+      }
+      __threadfence();
+      __syncthreads();
       if (tid == 0) {
         atomicExch(a.err, 1);
-        const double nan = __longlong_as_double(0x7ff8000000000000LL);
         for (int r = 0; r < 4; r++)
           if (J.rec[r].q >= 0 && J.rec[r].nrec > 0) J.rec[r].P[J.rec[r].rec0] = make_double2(nan, nan);
         for (int k = J.save_begin; k < J.save_end; k++)

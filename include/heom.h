@@ -111,8 +111,10 @@ typedef struct {
   int autotune;     /* 1 = time candidate launch shapes at plan creation */
   int single_pass;  /* 1 = propagate every scan point from t_start in one pass; 0 = stage
                        the scan (shared R/D2 per (tau1, tau2) group, per-point pulse-3
-                       windows, pulse-free tails two points per CTA) where the problem
-                       allows it -- bit-identical results */
+                       windows, FP64 jumps over pulse-free gaps, pulse-free tails as FP64
+                       dual dot products) where the problem allows it.  The two agree up
+                       to rounding, not bit for bit: jumps and dual tails round
+                       differently from step-by-step propagation */
 } heom_opts;
 
 /* Device plan: uploads H, X[0..3], the ADO neighbour tables and the bath
@@ -140,9 +142,13 @@ int heom_run_populations(heom_plan *plan, const int *sites, int n_sites, double 
 int heom_run_2des(heom_plan *plan, double *P, double *p_traj, int cap, int *n_out);
 
 /* A 2DES delay scan: n independent points (pulse times and end time replace the
- * key file's), the whole scan in one persistent kernel launch replayed from a CUDA
- * graph (replaces one CPU_2DES/GPU_2DES process per key file,
- * script/cpu-script/submit_jobs.sh:49-67).  Output of point i: counts[i] combined
+ * key file's) in one batched GPU run (replaces one CPU_2DES/GPU_2DES process per key
+ * file, script/cpu-script/submit_jobs.sh:49-67).  The default staged form plans its
+ * job queue on the host and then issues two plain launches: one persistent kernel over
+ * the queue (shared stages, pulse windows and jumps) and the pulse-free tail kernel;
+ * the per-sample block powers are formed on the first run after a sample changes.
+ * With heom_opts.single_pass = 1 the scan is one persistent kernel launch (after an
+ * ordering kernel) replayed from a CUDA graph.  Output of point i: counts[i] combined
  * P points at P + 2*offsets[i].  heom_scan_layout fills counts/offsets and returns
  * the total number of complex points through *total. */
 typedef struct { double tau1, tau2, tau3; float t_end; int flags; } heom_scan_point;
@@ -152,9 +158,25 @@ int heom_run_scan(heom_plan *plan, const heom_scan_point *pts, int n, double *P,
                   const long long *offsets, const int *counts);
 /* Same with every buffer already in device memory.  A staged scan reads the points and
  * offsets back once to plan its stages (one host synchronisation); a single-pass scan
- * does not synchronise. */
+ * does not synchronise.  Errors found on the device (a dependency wait that expired, a
+ * failed device-side check) are deferred: the call returns once the work is queued, and
+ * the status reaches the caller through heom_plan_sync, or else through the plan's next
+ * scan call.  The outputs of a failed run hold NaN where they depend on the failure. */
 int heom_run_scan_device(heom_plan *plan, const heom_scan_point *d_pts, int n, double *d_P,
                          const long long *d_offsets);
+/* Waits for the plan's queued work and returns the deferred status of its last
+ * heom_run_scan_device call: HEOM_ERR_TIMEOUT when a dependency wait of the staged scan
+ * expired, HEOM_ERR_CUDA when a device-side check failed or the stream reports an error.
+ * No counterpart in the reference, whose errors exit the process
+ * (etoheom-gpu/lib/HEOM_utilize.h:23-38). */
+int heom_plan_sync(heom_plan *plan);
+/* Test hook for the bounded device-side waits; no counterpart in the reference.  For the
+ * plan's next staged scan only, the dependency wait limit becomes wait_ns (default 30 s;
+ * at most 60 s), and with unmet != 0 the first job that waits on another job waits for a
+ * flag value that no producer sets.  That wait expires after wait_ns: the kernel writes
+ * NaN to the job's first records, releases the jobs that wait on it, and the run reports
+ * HEOM_ERR_TIMEOUT.  Every memory access stays in bounds; the next run is unaffected. */
+int heom_plan_inject_wait_fault(heom_plan *plan, unsigned long long wait_ns, int unmet);
 
 /* Delay scan that performs no device allocation, for callers that cannot let a library
  * allocate device memory (a service that reserves its whole budget at start-up in its own

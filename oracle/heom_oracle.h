@@ -55,6 +55,12 @@ int ho_traj(ho_problem *p, int nv1, int nv2, int nv3, int mode, int max_steps,
  * traj (optional) receives [n_sample][3][cap] complex points. */
 int ho_2des(ho_problem *p, int mode, int max_steps, double *P, int cap, int *npts, double *traj);
 
+/* ho_2des with the propagation, trace and combination in IEEE binary128 on the
+ * reference's double-precision problem data: the true result of the reference's
+ * discrete scheme (~1e-24 relative on the combined output), rounded to double.
+ * Same arguments as ho_2des (no mode: the RHS is the structured form). */
+int ho_2des_q(ho_problem *p, int max_steps, double *P, int cap, int *npts, double *traj);
+
 #ifdef __cplusplus
 }
 #endif

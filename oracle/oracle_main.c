@@ -1,7 +1,8 @@
 /* heom_oracle CLI -- TEST INFRASTRUCTURE ONLY.
  * Prints the same sections as oracle/ref_driver so the restatement can be
  * diffed against the reference's own code:
- *   heom_oracle <file.key> [--structured] [--max-steps N] [--single-manifold] */
+ *   heom_oracle <file.key> [--structured | --quad] [--max-steps N] [--single-manifold]
+ * --quad propagates and combines in binary128 (ho_2des_q). */
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -9,14 +10,15 @@
 
 int main(int argc, char **argv) {
   if (argc < 2) {
-    fprintf(stderr, "usage: %s <file.key> [--structured] [--max-steps N] [--single-manifold]\n", argv[0]);
+    fprintf(stderr, "usage: %s <file.key> [--structured | --quad] [--max-steps N] [--single-manifold]\n", argv[0]);
     return 2;
   }
-  int mode = HO_DENSE, max_steps = 0, single = 0;
+  int mode = HO_DENSE, max_steps = 0, single = 0, quad = 0;
   for (int a = 2; a < argc; a++) {
     if (!strcmp(argv[a], "--structured")) mode = HO_STRUCTURED;
     else if (!strcmp(argv[a], "--max-steps") && a + 1 < argc) max_steps = atoi(argv[++a]);
     else if (!strcmp(argv[a], "--single-manifold")) single = 1;
+    else if (!strcmp(argv[a], "--quad")) quad = 1;
   }
   ho_problem *p = NULL;
   char err[512];
@@ -29,7 +31,7 @@ int main(int argc, char **argv) {
   int cap = info[7] + 1, ns = info[6], n = 0;
   double *P = calloc(2 * (size_t)cap, sizeof(double));
   double *traj = calloc(2 * (size_t)cap * 3 * ns, sizeof(double));
-  if (ho_2des(p, mode, max_steps, P, cap, &n, traj)) {
+  if (quad ? ho_2des_q(p, max_steps, P, cap, &n, traj) : ho_2des(p, mode, max_steps, P, cap, &n, traj)) {
     fprintf(stderr, "error: propagation failed\n");
     return 1;
   }

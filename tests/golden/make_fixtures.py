@@ -158,6 +158,9 @@ def write_keys():
     H, dip = aggregate(7, 2024, 12400, 200, 100)
     files["c1_fmo.key"] = key_text(8, 7, 3, H, OHMIC_35_106_77K, dip,
                                    [(50, 20, 12500), (150, 20, 12500), (250, 20, 12500)], (0, 2000, 0.5, 0.5))
+    # c1 through all three pulse windows (601 steps, records from pulse 3 at 250 fs).
+    files["c1_fmo_300fs.key"] = key_text(8, 7, 3, H, OHMIC_35_106_77K, dip,
+                                         [(50, 20, 12500), (150, 20, 12500), (250, 20, 12500)], (0, 300, 0.5, 0.5))
     files["c1_fmo_short.key"] = key_text(8, 7, 3, H, OHMIC_35_106_77K, dip,
                                          [(0, 20, 12500), (1, 20, 12500), (0, 20, 12500)], (0, 3, 0.5, 0.5))
     # c3: 12-site chain, single-excitation manifold (extension keyword), L=3.
@@ -229,7 +232,8 @@ def parse_driver_output(text):
 
 DYNAMICS = ["d_dimer.key", "d_trimer.key"]
 GOLDEN = ["c0_dimer_short.key", "c0_dimer.key", "c4_trimer_short.key", "t_disorder.key",
-          "t_ref_example.key", "t_strong.key", "c1_fmo_short.key"]
+          "t_ref_example.key", "t_strong.key", "c1_fmo_short.key",
+          "c1_fmo_300fs.key"]   # the last one is ~12 min of CPU (dense N = 29 zgemm)
 
 
 # The delay scan of the heom_scan driver test (gen_2d_data.sh parameters).
@@ -297,10 +301,129 @@ def write_golden():
     print(f"scan: {len(keys)} CPU_2DES outputs")
 
 
+def scan_key_text(row):
+    """The c2 scan template with one point's pulse times and end time."""
+    text = open(os.path.join(KEYS, "c2_dimer_scan.key-tmpl")).read()
+    r = [repr(float(v)) for v in row[:4]]
+    return text.replace("TAU1", r[0]).replace("TAU2", r[1]).replace("TAU3", r[2]).replace("T_END", r[3])
+
+
+def truth_points():
+    """Stratified subset of the 1024-point c2 scan: for each of rephasing / non-rephasing
+    and each of the 8 waiting times, 3 coherence times drawn from a fixed seed (the
+    shortest, t1 = 0, at T = 0 and the longest, t1 = 315 fs, at T = 700 fs forced in).
+    Returns [(grid index, (tau1, tau2, tau3, t_end))]."""
+    grid = scan_points()
+    rng = np.random.default_rng(2026)
+    out = []
+    for ik, kind in enumerate(("R", "NR")):
+        for i2 in range(8):
+            idx = sorted(int(v) for v in rng.choice(64, 3, replace=False))
+            if i2 == 0:
+                idx[0] = 0
+            if i2 == 7:
+                idx[-1] = 63
+            for i1 in sorted(set(idx)):
+                g = (ik * 8 + i2) * 64 + i1
+                assert grid[g][4] == kind
+                out.append((g, grid[g][:4]))
+    return out
+
+
+def short_scan_rows(t0=50.0, t1s=(0.0, 35.0, 80.0, 155.0), t2s=(0.0, 100.0, 300.0), t3=150.0):
+    """The shortened scan geometry of the GPU scan tests (t3 = 150 fs)."""
+    rows = []
+    for t2 in t2s:
+        for t1 in t1s:
+            rows.append((t0, t0 + t1, t0 + t1 + t2, t0 + t1 + t2 + t3))   # rephasing
+            rows.append((t0 + t1, t0, t0 + t1 + t2, t0 + t1 + t2 + t3))   # non-rephasing
+    return rows
+
+
+def _run_point(args):
+    exe, text, extra = args
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        kp = os.path.join(d, "p.key")
+        with open(kp, "w") as f:
+            f.write(text)
+        out = subprocess.run([exe, kp, *extra], check=True, capture_output=True, text=True).stdout
+    return parse_driver_output(out)
+
+
+def write_truth(workers=None):
+    """Binary128 truth (heom_oracle --quad: the reference's scheme on its own double
+    data, propagated and combined in binary128) for
+      * truth_c2.npz: the stratified 48-point subset of the c2 scan at full length
+        (t3 = 400 fs), with the reference build's own double result beside it;
+      * truth_scan_short.npz: the 24-point shortened scan of the GPU scan tests;
+      * truth_c0_dimer_short.npz: the c0 short point of the smoke check.
+    About 30 s of CPU per full-length point; points run in parallel processes."""
+    from concurrent.futures import ThreadPoolExecutor
+    oracle_exe = os.path.join(ROOT, "oracle", "heom_oracle")
+    ref_exe = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    for exe, tgt in ((oracle_exe, "all"), (ref_exe, "ref")):
+        if not os.path.exists(exe):
+            subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), tgt])
+    workers = workers or max(1, (os.cpu_count() or 2) - 1)
+
+    def pack(rows, results):
+        counts = [len(c) for _, c in results]
+        off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        return np.array(rows, dtype=np.float64), off, np.concatenate([c for _, c in results])
+
+    sets = {"c2": [r for _, r in truth_points()], "scan_short": short_scan_rows()}
+    with ThreadPoolExecutor(workers) as ex:
+        for name, rows in sets.items():
+            jobs = [(oracle_exe, scan_key_text(r), ["--quad"]) for r in rows]
+            truth = list(ex.map(_run_point, jobs))
+            R, off, P = pack(rows, truth)
+            extra = {}
+            if name == "c2":
+                extra["grid_index"] = np.array([g for g, _ in truth_points()], dtype=np.int64)
+                ref = list(ex.map(_run_point, [(ref_exe, scan_key_text(r), []) for r in rows]))
+                R2, off2, Pref = pack(rows, ref)
+                assert np.array_equal(off, off2)
+                extra["reference"] = Pref
+            np.savez_compressed(os.path.join(REF, f"truth_{name}.npz"), rows=R, offsets=off, truth=P, **extra)
+            print(f"truth_{name}: {len(rows)} points, {len(P)} records")
+    write_truth_keys(workers)
+
+
+TRUTH_KEYS = ["c0_dimer_short.key", "c4_trimer_short.key", "t_disorder.key"]
+
+
+def write_truth_keys(workers=None):
+    """Binary128 truth of single key files (truth_<key>.npz: traj, combined) and of the
+    heom_scan driver's delay scan (truth_scan_driver.npz: one combined output per
+    out_{tau}_{T}.out file, disorder-averaged over the key's two samples)."""
+    from concurrent.futures import ThreadPoolExecutor
+    oracle_exe = os.path.join(ROOT, "oracle", "heom_oracle")
+    workers = workers or max(1, (os.cpu_count() or 2) - 1)
+    with ThreadPoolExecutor(workers) as ex:
+        res = list(ex.map(_run_point, [(oracle_exe, open(os.path.join(KEYS, k)).read(), ["--quad"])
+                                       for k in TRUTH_KEYS]))
+        for k, (traj, comb) in zip(TRUTH_KEYS, res):
+            np.savez_compressed(os.path.join(REF, "truth_" + k.replace(".key", ".npz")), traj=traj, combined=comb)
+            print(f"truth_{k}: {len(comb)} records")
+        keys = gen_2d_keys(open(os.path.join(KEYS, "t_scan.key-tmpl")).read(), **SCAN_ARGS)
+        names = sorted(keys)
+        res = list(ex.map(_run_point, [(oracle_exe, keys[n], ["--quad"]) for n in names]))
+        counts = [len(c) for _, c in res]
+        off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        outs = np.array(["out" + n[3:-4] + ".out" for n in names])
+        np.savez_compressed(os.path.join(REF, "truth_scan_driver.npz"), names=outs, offsets=off,
+                            truth=np.concatenate([c for _, c in res]))
+        print(f"truth_scan_driver: {len(names)} files")
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--golden", action="store_true")
+    ap.add_argument("--golden", action="store_true", help="golden vectors from the reference build (oracle/_ref)")
+    ap.add_argument("--truth", action="store_true", help="binary128 truth vectors (heom_oracle --quad)")
     a = ap.parse_args()
     print("\n".join(write_keys()))
     if a.golden:
         write_golden()
+    if a.truth:
+        write_truth()

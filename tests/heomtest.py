@@ -68,6 +68,7 @@ class Oracle:
         L.ho_rhs.argtypes = [P, D, D, D, I]
         L.ho_traj.argtypes = [P, I, I, I, I, I, D, I, ctypes.POINTER(I)]
         L.ho_2des.argtypes = [P, I, I, D, I, ctypes.POINTER(I), D]
+        L.ho_2des_q.argtypes = [P, I, D, I, ctypes.POINTER(I), D]
         self.L = L
 
     def load(self, path: str, single_manifold: bool = False):
@@ -137,6 +138,28 @@ class OracleProblem:
         rc = self.o.L.ho_2des(self.h, mode, max_steps, dp(P), cap, ctypes.byref(n), dp(tr))
         assert rc == 0
         return P[:n.value], tr[:, :, :n.value]
+
+
+    def run_2des_truth(self, max_steps=0):
+        """ho_2des_q: the reference's scheme in binary128 (the true combined output)."""
+        cap = self.n_steps + 1
+        P = np.zeros(cap, dtype=np.complex128)
+        tr = np.zeros((self.n_sample, 3, cap), dtype=np.complex128)
+        n = ctypes.c_int()
+        dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
+        rc = self.o.L.ho_2des_q(self.h, max_steps, dp(P), cap, ctypes.byref(n), dp(tr))
+        assert rc == 0
+        return P[:n.value], tr[:, :, :n.value]
+
+
+def truth(name: str):
+    """Binary128 truth fixture tests/golden/ref/truth_<name>.npz (make_fixtures.py --truth):
+    (rows, [P_true per point], [reference build P per point] or None, grid indices or None)."""
+    d = np.load(os.path.join(REF, f"truth_{name}.npz"))
+    off = d["offsets"]
+    cut = lambda a: [a[off[i]:off[i + 1]] for i in range(len(off) - 1)]  # noqa: E731
+    return (d["rows"], cut(d["truth"]), cut(d["reference"]) if "reference" in d else None,
+            d["grid_index"] if "grid_index" in d else None)
 
 
 _oracle = None

@@ -1,4 +1,4 @@
-"""Population dynamics on the GPU: dynamics_solver / CPU_dynamics.
+"""Population dynamics on the GPU: the dynamics_solver / CPU_dynamics replacement.
 
 The bit-exact FP64 path runs the reference's RK4 and right-hand side
 (total_ADO_dynamics, dynamics.cpp:52-115, which is total_ADO_dynamics_Ht with the static

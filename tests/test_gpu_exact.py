@@ -16,7 +16,9 @@ from heomtest import PKG_DIR, REF, golden, key, load_pkg, oracle, rel_err
 pytestmark = pytest.mark.gpu
 
 SMEM_KEYS = ["c0_dimer_short.key", "t_disorder.key", "t_ref_example.key", "t_strong.key"]
-STAGED_KEYS = ["c4_trimer_short.key", "c1_fmo_short.key"]
+# c1_fmo_300fs: the 7-site FMO aggregate (N = 29, 680 ADOs) through all three pulse
+# windows, 601 RK4 steps, against the reference build run here for ~12 min of CPU.
+STAGED_KEYS = ["c4_trimer_short.key", "c1_fmo_short.key", "c1_fmo_300fs.key"]
 
 
 def run_key(heom, name, precision="fp64-exact"):

@@ -2,15 +2,16 @@
 
 Accuracy gates (max_t |P - P_ref| / max_t |P_ref| per scan point, combined output):
   * FP32-bulk vs the FP64 scan path: <= 1e-6 (the FP32-bulk target);
-  * FP64 scan vs the reference's own arithmetic (bit-exact path): the combined output
-    of the reference is a ~1e-9 residue of per-trajectory values, so its own rounding
-    noise is ~1e-6 of it; the FP64 scan must agree to that noise floor (<= 1e-4), and
-    per-trajectory-scale agreement is checked separately on the linear signals.
+  * FP64 scan vs the reference's own arithmetic (bit-exact path): the reference's
+    combined output is a residue of per-trajectory values ~9 orders larger, so it
+    carries its own rounding noise, measured per point against the binary128 truth
+    (tests/golden/ref/truth_scan_short.npz).  The FP64 scan must lie within that noise
+    plus 1e-10; its own error against the truth is gated in test_gpu_truth.py.
 """
 import numpy as np
 import pytest
 
-from heomtest import key, load_pkg, rel_err
+from heomtest import key, load_pkg, rel_err, truth
 
 pytestmark = pytest.mark.gpu
 
@@ -63,15 +64,20 @@ def test_scan_fp32_vs_fp64(setup):
 def test_scan_fp64_vs_reference_arithmetic(setup, tmp_path_factory):
     heom, prob = setup
     rows = scan_geometry()[:6]
+    t_rows, t_want, _, _ = truth("scan_short")
+    assert np.array_equal(t_rows[:6], np.array(rows))
     pts = heom.make_points(rows)
     r64 = heom.Plan(prob, "fp64", max_points=len(rows)).run_scan(pts)
-    errs = []
+    errs, noise = [], []
     for i, row in enumerate(rows):
         ref = exact_point(heom, prob, row, tmp_path_factory)
         assert len(ref) == r64.counts[i]
         errs.append(rel_err(r64.point(i), ref))
+        noise.append(rel_err(ref, t_want[i]))
     print("fp64 scan vs reference arithmetic per point:", ["%.2e" % e for e in errs])
-    assert max(errs) <= 1e-4
+    print("reference arithmetic vs truth per point:   ", ["%.2e" % e for e in noise])
+    for e, n in zip(errs, noise):
+        assert e <= n * (1 + 1e-3) + 1e-10
 
 
 def test_scan_point_order_does_not_matter(setup):
