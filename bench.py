@@ -16,8 +16,10 @@ Also reported: the plain FP64 path (bit-exact, one point at a time) on a sample 
 points, the FP32-bulk error against the FP64 scan, the roofline of the scan kernel,
 GPU clocks during the timed region and the reference CPU build on a bounded sample.
 
-Multi-GPU (torchrun): every rank runs its own 1024-point scan (a different disorder
-sample), no collective on the data path; value = all points / max-over-ranks time.
+Multi-GPU (torchrun): every rank runs its own 1024-point scan of a different disorder /
+orientation sample (weak scaling), no collective on the data path; value = all points /
+max-over-ranks time.  After the timed region one gather (eto-heom_b200/shard.py, NCCL)
+brings the ranks' P(t) to rank 0, which forms the disorder average as CPU_2DES does.
 """
 from __future__ import annotations
 
@@ -117,6 +119,16 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def measured_peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -192,7 +204,10 @@ def run_reference_arm(a):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": {"workload": "c2 dimer 2DES delay scan (1024 points), reference CPU build",
                                         "points_per_step": per_step},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "cpu_model": cpu_model(), "kind": kind,
+                         "sample": sample + "; the rate over this sample stands for the whole 1024-point scan "
+                                            "(an extrapolation: the sample is stratified over the scan's "
+                                            "point lengths)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -249,6 +264,48 @@ def large_n_record(heom, device: int, fp32_peak: float) -> dict:
                       "frac": ab / fp32_peak, "rel_err_vs_exact": rel_err(Pb, Px),
                       "note": "four mixed-difference components per step (general-size staged path)"},
     }
+
+
+def adjoint_record(heom, device: int) -> dict:
+    """Config 4 at its stated size: the trimer (N = 7, 210 ADOs) rephasing P(t1, t3) on
+    32 t1 x 128 t3 at t2 = 200 fs, L2 loss against the target of the Hamiltonian
+    parameters perturbed by 2 %, gradient of the 12 parameters by the checkpointed
+    adjoint (heom_adjoint_scan).  Wall time of one FP64 forward scan and of one gradient
+    (forward with checkpoints, recomputed segments and the adjoint sweep)."""
+    import importlib
+    import math
+
+    from make_fixtures import c4_fit_rows
+
+    ag = importlib.import_module("eto_heom_b200.autograd")
+    prob = heom.Problem.from_key(os.path.join(ROOT, "tests", "golden", "keys", "c4_trimer_fit.key"))
+    prob.prepare_sample()
+    params = ag.ScanParameters(prob)
+    rows = c4_fit_rows()
+    pts = heom.make_points(rows)
+    th0 = params.theta0.copy()
+    th_t = th0.copy()
+    th_t[:params.n_h] *= 1.02
+    params.apply(th_t)
+    target = heom.Plan(prob, "fp64", device=device, max_points=len(pts)).run_scan(pts).P
+    params.apply(th0)
+    plan = heom.Plan(prob, "fp64", device=device, max_points=len(pts))
+    plan.run_scan(pts)
+    t0 = time.perf_counter()
+    P = plan.run_scan(pts).P
+    t_fwd = time.perf_counter() - t0
+    g = 2.0 * (P - target)
+    plan.adjoint_scan(pts, g)
+    t0 = time.perf_counter()
+    _, grad = plan.adjoint_scan(pts, g)
+    t_adj = time.perf_counter() - t0
+    steps = max(steps_of(r[3]) for r in rows)
+    return {"workload": "c4 trimer fit: N=7, 210 ADOs, rephasing 32 t1 x 128 t3 at t2 = 200 fs, 12 parameters",
+            "records": int(len(P)), "max_rk4_steps": steps, "checkpoint_interval": int(math.ceil(math.sqrt(steps))),
+            "forward_ms": 1e3 * t_fwd, "gradient_ms": 1e3 * t_adj, "loss": float(np.sum(np.abs(g / 2) ** 2)),
+            "grad_norm": float(np.linalg.norm(grad)),
+            "note": "FP64 mixed-difference basis; checked against Richardson-extrapolated central "
+                    "differences (h = 1e-4 relative) in tests/test_gpu_adjoint_c4.py"}
 
 
 def run_ours(a):
@@ -320,6 +377,18 @@ def run_ours(a):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = world * n / (ms / 1e3)
+    averaged = None
+    if dist:
+        # the disorder average of the ranks' samples (CPU_2DES.cpp:83-89) on rank 0: one
+        # gather of every rank's P(t) through the shard module (NCCL), outside the timed region
+        import importlib
+        shard = importlib.import_module("eto_heom_b200.shard")
+        torch.cuda.synchronize()
+        mine = d_P.cpu().numpy().view(np.complex128).copy()
+        parts = shard.gather_to_rank0(mine, rank, world, device=torch.device("cuda", local))
+        if rank == 0:
+            avg = np.mean(np.stack(parts), axis=0)
+            averaged = {"samples": world, "records": int(len(avg)), "finite": bool(np.isfinite(avg).all())}
 
     # kernel-only duration (CUDA events around the scan kernel alone are the same
     # graph; the order kernel is ~10 us), roofline of the scan kernel
@@ -377,6 +446,24 @@ def run_ours(a):
         cpu_val, kind, wall, _ = reference_cpu(rows, cores, cores)
         clocks = clk.summary()
         large_n = large_n_record(heom, local, peak)
+        adjoint = adjoint_record(heom, local)
+        # cold-sample e2e: a new disorder/orientation sample before every scan
+        # (heom_problem_prepare_sample + heom_plan_update + heom_run_scan), so the per-sample
+        # set-up -- T0 and its squares on the GPU, the dual tail rows on the host -- falls
+        # inside the timed region.  Run last: it moves the problem to new samples.
+        cold_t = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            prob.prepare_sample()
+            plan.update()
+            plan.run_scan(pts, (pts, off, cnt, tot))
+            cold_t.append(time.perf_counter() - t0)
+        warm_s = float(np.mean(e2e_t[1:] if len(e2e_t) > 1 else e2e_t))
+        e2e_cold = {"value": n / float(np.mean(cold_t)), "unit": UNIT,
+                    "h2d_bytes_per_step": int(pts.nbytes + off.nbytes), "d2h_bytes_per_step": int(16 * tot),
+                    "setup_ms_per_sample": 1e3 * (float(np.mean(cold_t)) - warm_s),
+                    "note": "a new disorder/orientation sample every step: prepare_sample + plan.update + "
+                            "run_scan through the host-buffer C ABI; setup = cold minus warm e2e time"}
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -389,6 +476,7 @@ def run_ours(a):
                        "launch": plan.describe(), "parallelism": f"dp{world} (independent scans)"},
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(pts.nbytes + off.nbytes),
                     "d2h_bytes_per_step": int(16 * tot)},
+            "e2e_cold": e2e_cold,
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
@@ -405,12 +493,16 @@ def run_ours(a):
             "plain_fp64": {"value": plain_val, "unit": UNIT, "sample": f"{len(sample_idx)} points, one at a time, "
                            "bit-exact FP64 path, scaled to the scan by RK4 step count",
                            "speedup_of_chosen": value / plain_val},
-            "cpu_baseline": {"value": cpu_val, "unit": UNIT, "cores": cores, "kind": kind,
+            "cpu_baseline": {"value": cpu_val, "unit": UNIT, "cores": cores, "cpu_model": cpu_model(), "kind": kind,
                              "sample": f"{cores} stratified scan points, one CPU_2DES process each, "
-                                       f"{cores} concurrent ({wall:.1f} s)"},
+                                       f"{cores} concurrent ({wall:.1f} s); extrapolated to the 1024-point "
+                                       "scan as points per second over the sample"},
             "clocks": clocks,
             "large_n": large_n,
+            "adjoint_c4": adjoint,
         }
+        if averaged:
+            out["disorder_average"] = averaged
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()
@@ -424,6 +516,8 @@ def profile_run(precision: str):
     fp32-bulk / fp64: the first 148 points of the dimer scan (one per SM) with t3
     shortened to 50 fs, default launch shape, one run of the scan kernel.
     fp32-bulk-tails: all 1024 points with t3 = 100 fs (the tail kernel's full grid).
+    fp32-bulk-full: the bench's 1024-point scan, run twice (the second run is the bench's
+    steady state: T0 and its powers are cached on the plan).
     c1-*: one 2DES point of the FMO key (N = 8, 680 ADOs) with the pulses at 10, 20 and
     30 fs (5 fs wide) and the end at 40 fs -- 81 RK4 steps of the general-size staged
     path (c1-fp32-bulk, c1-fp64) or of the bit-exact path (c1-fp64-exact)."""
@@ -455,6 +549,14 @@ def profile_run(precision: str):
         return
     prob = heom.Problem.from_key(KEY)
     prob.prepare_sample()
+    if precision == "fp32-bulk-full":  # the bench's own 1024-point scan, run twice (T0 powers cached)
+        plan = heom.Plan(prob, "fp32-bulk", max_points=1024)
+        pts = heom.make_points(scan_rows())
+        for _ in range(2):
+            r = plan.run_scan(pts)
+        torch.cuda.synchronize()
+        print(f"profile run: 1024 points, {len(r.P)} P values, {plan.describe()}")
+        return
     if precision == "fp32-bulk-tails":  # every point, t3 = 100 fs: the tail kernel's full grid
         rows = [(a, b, c, c + 100.0) for a, b, c, _ in scan_rows()]
         precision = "fp32-bulk"
@@ -472,7 +574,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--profile-run", default=None, choices=["fp32-bulk", "fp64", "fp32-bulk-tails", "c1-fp32-bulk", "c1-fp64", "c1-fp64-exact"],
+    ap.add_argument("--profile-run", default=None, choices=["fp32-bulk", "fp64", "fp32-bulk-tails", "fp32-bulk-full", "c1-fp32-bulk", "c1-fp64",
+                             "c1-fp64-exact"],
                     help="run only a small scan of that precision (for profiler captures)")
     a = ap.parse_args()
     if a.profile_run:

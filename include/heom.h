@@ -182,15 +182,19 @@ int heom_plan_inject_wait_fault(heom_plan *plan, unsigned long long wait_ns, int
  * allocate device memory (a service that reserves its whole budget at start-up in its own
  * pool or an ML framework's caching allocator, or an application that allows allocation
  * only during initialisation).  No counterpart in the reference.  Same computation as
- * heom_run_scan_device with the default launch shape, on the caller's current device and
- * the given stream (NULL = legacy default stream); inputs and outputs are the caller's
- * device buffers, the problem comes from the host handle.  Its scratch (work-queue
- * counter, point ordering, packed tables and system matrices) lives in one 4 MiB
- * file-scope device array that every GPU loading the library holds until exit: at most
- * 65536 points per call, and the problem's tables must fit (else HEOM_ERR_CAPACITY).
- * All calls on a device share that array; calls whose GPU work overlaps race and must be
- * serialised by the caller.  The first call on a device resolves the array's address;
- * make it before any stream capture on that device.  Asynchronous: no synchronisation. */
+ * the single-pass form of heom_run_scan_device (heom_opts.single_pass = 1; a staged plan
+ * agrees with it to rounding) with the default launch shape, on the caller's current
+ * device and the given stream (NULL = legacy default stream); inputs and outputs are the
+ * caller's device buffers, the problem comes from the host handle.  Its scratch
+ * (work-queue counter, point ordering, packed tables and system matrices) lives in one
+ * 4 MiB file-scope device array that every GPU loading the library holds until exit: at
+ * most 65536 points per call, and the problem's tables must fit (else
+ * HEOM_ERR_CAPACITY).  All calls on a device share that array; calls whose GPU work
+ * overlaps race and must be serialised by the caller.  The first call on a device
+ * resolves the array's address.  The tables are uploaded from host memory that the call
+ * owns (pageable copies), so the call waits for earlier work on the stream before it
+ * returns, and it must not be captured into a CUDA graph.  The scan itself is queued
+ * and runs asynchronously. */
 int heom_run_scan_noalloc(const heom_problem *p, int precision, const heom_scan_point *d_pts, int n,
                           double *d_P, const long long *d_offsets, void *stream);
 

@@ -173,6 +173,9 @@ def write_keys():
     H, dip = aggregate(3, 4, 0, 0, 120, e_fixed=[12300, 12450, 12600])
     files["c4_trimer.key"] = key_text(4, 3, 4, H, OHMIC_35_106_77K, dip,
                                       [(50, 20, 12500), (150, 20, 12500), (350, 20, 12500)], (0, 1000, 0.5, 0.5))
+    # c4 fit workload: P(t1, t3) recorded every 2 fs (128 t3 samples per point over 254 fs)
+    files["c4_trimer_fit.key"] = key_text(4, 3, 4, H, OHMIC_35_106_77K, dip,
+                                          [(50, 20, 12500), (150, 20, 12500), (350, 20, 12500)], (0, 1000, 0.5, 2))
     files["c4_trimer_short.key"] = key_text(4, 3, 4, H, OHMIC_35_106_77K, dip,
                                             [(20, 20, 12500), (50, 20, 12500), (80, 20, 12500)], (0, 160, 0.5, 0.5))
     # Disorder + several samples: exercises the RNG stream, the diagonal sort and averaging.
@@ -328,6 +331,17 @@ def truth_points():
                 assert grid[g][4] == kind
                 out.append((g, grid[g][:4]))
     return out
+
+
+def c4_fit_rows(t0=50.0, n_t1=32, t1_step=5.0, t2=200.0, t3_span=255.0):
+    """The config-4 grid: rephasing points t1 = 0..155 fs at t2 = 200 fs; with records
+    every 2 fs from pulse 3 on, t_end = tau3 + 255 fs gives 128 t3 samples per point."""
+    rows = []
+    for i in range(n_t1):
+        t1 = i * t1_step
+        tau3 = t0 + t1 + t2
+        rows.append((t0, t0 + t1, tau3, tau3 + t3_span))
+    return rows
 
 
 def short_scan_rows(t0=50.0, t1s=(0.0, 35.0, 80.0, 155.0), t2s=(0.0, 100.0, 300.0), t3=150.0):

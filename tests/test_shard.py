@@ -24,6 +24,28 @@ def test_lpt_partition_balances_and_covers():
     assert max(loads) - min(loads) <= max(work)
 
 
+def test_partition_keeps_groups_whole_and_balances():
+    import importlib
+    import sys
+
+    heom = load_pkg()
+    shard = importlib.import_module("eto_heom_b200.shard")
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_fixtures import scan_points
+    pts = heom.make_points([(a, b, c, d) for a, b, c, d, _ in scan_points()])
+    groups = shard.scan_groups(pts)
+    assert len(groups) == 127 and sum(len(g) for g in groups) == 1024   # t1 = 0: R and NR coincide
+    for world in (2, 4, 8):
+        parts = shard.partition_groups(pts, world)
+        assert sorted(i for p in parts for i in p) == list(range(1024))
+        owner = {i: r for r, p in enumerate(parts) for i in p}
+        for g in groups:   # every group on one rank
+            assert len({owner[i] for i in g}) == 1
+        w = [shard.group_work(pts, g) for g in groups]
+        loads = [sum(w[gi] for gi, g in enumerate(groups) if owner[g[0]] == r) for r in range(world)]
+        assert max(loads) - min(loads) <= max(w)
+
+
 def _points(n):
     heom = load_pkg()
     rows = [(50.0, 50.0 + 5 * i, 60.0 + 5 * i, 100.0 + 7 * (i % 11)) for i in range(n)]
