@@ -1394,6 +1394,7 @@ static void dual_operator(ScanState &s, const std::vector<double> &sys, const st
   }
   s.W_rows = 1;
   s.W_dev_rows = 0;
+  s.dual_dirty = true;
   s.dual_pos = pos;
   s.dual_pos_dirty = true;
 }
@@ -1455,10 +1456,18 @@ static void jump_operator(ScanState &s, const std::vector<double> &sys) {
 }
 
 // C = ident * I + alpha * A B for square d x d complex FP64 matrices (row-major): the
-// Horner steps of T0 = T4(h L0) and the squarings T0^(2^(j+1)) = (T0^(2^j))^2.
-__global__ void jump_gemm(int d, double alpha, int ident, const double2 *__restrict__ A,
-                          const double2 *__restrict__ B, double2 *__restrict__ C) {
+// Horner steps of T0 = T4(h L0) and the squarings T0^(2^(j+1)) = (T0^(2^j))^2.  One
+// launch covers every position block: blockIdx.z is the block, whose size and offset
+// (in elements, the same for A, B and C) come from dims / offs; tiles outside a block
+// return at once.
+__global__ void jump_gemm(const int *__restrict__ dims, const long long *__restrict__ offs, double alpha, int ident,
+                          const double2 *__restrict__ A0, const double2 *__restrict__ B0, double2 *__restrict__ C0) {
   __shared__ double2 As[16][17], Bs[16][17];
+  const int d = dims[blockIdx.z];
+  if ((int)blockIdx.y * 16 >= d || (int)blockIdx.x * 16 >= d) return;
+  const long long o = offs[blockIdx.z];
+  const double2 *A = A0 + o, *B = B0 + o;
+  double2 *C = C0 + o;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int row = blockIdx.y * 16 + ty, col = blockIdx.x * 16 + tx;
   double re = 0.0, im = 0.0;
@@ -1479,21 +1488,35 @@ __global__ void jump_gemm(int d, double alpha, int ident, const double2 *__restr
 }
 
 // Powers T0^(2^j), j < need, of every jump block on the device (cached per sample).
+// Buffers are kept across samples while the block structure needs no more room.
 static int jump_powers(ScanState &s, int need, cudaStream_t st) {
   cudaError_t e = cudaSuccess;
   const size_t pe = (size_t)s.jpow_elems;
+  const int nb = s.jtab[0];
   if (s.jL_dirty) {
-    if (s.d_jtab) cudaFree(s.d_jtab);
-    if (s.d_jL) cudaFree(s.d_jL);
-    if (s.d_jtmp) cudaFree(s.d_jtmp);
-    s.d_jtab = s.d_jL = s.d_jtmp = nullptr;
-    e = cudaMalloc(&s.d_jtab, sizeof(int) * s.jtab.size());
-    if (e == cudaSuccess) e = cudaMalloc(&s.d_jL, sizeof(double2) * pe);
-    if (e == cudaSuccess) e = cudaMalloc(&s.d_jtmp, 2 * sizeof(double2) * pe);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(s.d_jtab, s.jtab.data(), sizeof(int) * s.jtab.size(), cudaMemcpyHostToDevice, st);
+    const size_t meta = sizeof(int) * s.jtab.size() + 256 + sizeof(long long) * nb;
+    if (pe > s.jL_cap || meta > s.jtab_cap) {
+      if (s.d_jtab) cudaFree(s.d_jtab);
+      if (s.d_jL) cudaFree(s.d_jL);
+      if (s.d_jtmp) cudaFree(s.d_jtmp);
+      s.d_jtab = s.d_jL = s.d_jtmp = nullptr;
+      s.jL_cap = s.jtab_cap = 0;
+      e = cudaMalloc(&s.d_jtab, meta);
+      if (e == cudaSuccess) e = cudaMalloc(&s.d_jL, sizeof(double2) * pe);
+      if (e == cudaSuccess) e = cudaMalloc(&s.d_jtmp, 2 * sizeof(double2) * pe);
+      if (e == cudaSuccess) { s.jL_cap = pe; s.jtab_cap = meta; }
+    }
+    // [jtab][pad to 256][per-block element offsets]; jump_gemm reads dims from jdims below
+    s.h_jmeta.assign(meta, 0);
+    std::memcpy(s.h_jmeta.data(), s.jtab.data(), sizeof(int) * s.jtab.size());
+    const size_t off_offs = (sizeof(int) * s.jtab.size() + 255) & ~(size_t)255;
+    for (int b = 0; b < nb; b++) {
+      const long long o = s.jtab[1 + 2 * nb + b];
+      std::memcpy(s.h_jmeta.data() + off_offs + sizeof(long long) * b, &o, sizeof o);
+    }
+    s.jmeta_offs = off_offs;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_jtab, s.h_jmeta.data(), meta, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_jL, s.h_jL.data(), sizeof(double2) * pe, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     s.jpow_n = 0;
     s.jL_dirty = false;
   }
@@ -1507,35 +1530,171 @@ static int jump_powers(ScanState &s, int need, cudaStream_t st) {
   }
   if (e != cudaSuccess) { s_err = std::string("jump tables: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
   double2 *L = (double2 *)s.d_jL, *P = (double2 *)s.d_jpow, *X0 = (double2 *)s.d_jtmp, *X1 = X0 + pe;
-  const int nb = s.jtab[0];
-  auto gemm = [&](int d, double alpha, int ident, const double2 *A, const double2 *B, double2 *C) {
-    const dim3 g((d + 15) / 16, (d + 15) / 16), t(16, 16);
-    jump_gemm<<<g, t, 0, st>>>(d, alpha, ident, A, B, C);
-  };
-  for (int j = s.jpow_n; j < need; j++)
-    for (int b = 0; b < nb; b++) {
-      const int d = s.jdims[b];
-      const size_t o = (size_t)s.jtab[1 + 2 * nb + b];
-      if (j == 0) { // Horner: X = I; X = I + (h/m) L X, m = 4..1
-        gemm(d, 0.0, 1, L + o, L + o, X0 + o);
-        gemm(d, s.h / 4, 1, L + o, X0 + o, X1 + o);
-        gemm(d, s.h / 3, 1, L + o, X1 + o, X0 + o);
-        gemm(d, s.h / 2, 1, L + o, X0 + o, X1 + o);
-        gemm(d, s.h, 1, L + o, X1 + o, P + o);
-      } else {
-        gemm(d, 1.0, 0, P + (j - 1) * pe + o, P + (j - 1) * pe + o, P + j * pe + o);
-      }
+  // block sizes (rows) are jtab's position counts times n_ado: the dims table is the
+  // position counts, scaled here on the host into a second small upload
+  int dmax = 0;
+  for (int b = 0; b < nb; b++) dmax = std::max(dmax, s.jdims[b]);
+  if (s.h_jdims.size() != (size_t)nb || !std::equal(s.h_jdims.begin(), s.h_jdims.end(), s.jdims.begin())) {
+    s.h_jdims = s.jdims;
+    if (nb > s.jdims_cap) {
+      if (s.d_jdims) cudaFree(s.d_jdims);
+      s.d_jdims = nullptr;
+      s.jdims_cap = 0;
+      e = cudaMalloc(&s.d_jdims, sizeof(int) * nb);
+      if (e == cudaSuccess) s.jdims_cap = nb;
     }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_jdims, s.h_jdims.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) { s_err = std::string("jump dims: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  }
+  const int *dims = (const int *)s.d_jdims;
+  const long long *offs = (const long long *)((const unsigned char *)s.d_jtab + s.jmeta_offs);
+  const dim3 g((dmax + 15) / 16, (dmax + 15) / 16, nb), t(16, 16);
+  auto gemm = [&](double alpha, int ident, const double2 *A, const double2 *B, double2 *C) {
+    jump_gemm<<<g, t, 0, st>>>(dims, offs, alpha, ident, A, B, C);
+  };
+  for (int j = s.jpow_n; j < need; j++) {
+    if (j == 0) { // Horner: X = I; X = I + (h/m) L X, m = 4..1
+      gemm(0.0, 1, L, L, X0);
+      gemm(s.h / 4, 1, L, X0, X1);
+      gemm(s.h / 3, 1, L, X1, X0);
+      gemm(s.h / 2, 1, L, X0, X1);
+      gemm(s.h, 1, L, X1, P);
+    } else {
+      gemm(1.0, 0, P + (j - 1) * pe, P + (j - 1) * pe, P + j * pe);
+    }
+  }
   e = cudaGetLastError();
   if (e != cudaSuccess) { s_err = std::string("jump powers: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
   s.jpow_n = std::max(s.jpow_n, need);
   return 0;
 }
 
+// The dual vectors on the device: rows k0 .. rows-1 of W, w_{k+1} = T4(h L^T) w_k in
+// Horner form (u = w + (h/m) L^T u, m = 4..1), FP64, with L^T in CSR (start, idx, coef).
+// One CTA walks the chain; w and u live in shared memory, each thread keeps the new
+// values of its cells in registers across the barrier that separates reads from writes.
+constexpr int kDualRowThreads = 256;
+constexpr int kDualRowCells = 4; // cells per thread: at most kDualRowThreads * kDualRowCells cells
+
+__global__ void __launch_bounds__(kDualRowThreads) dual_rows_kernel(int cells, const int *__restrict__ start,
+                                                                    const int *__restrict__ idx,
+                                                                    const double2 *__restrict__ coef, double h,
+                                                                    double2 *__restrict__ W, int k0, int rows) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  double2 *w = (double2 *)sm, *u = w + cells;
+  const int tid = threadIdx.x;
+  for (int c = tid; c < cells; c += blockDim.x) w[c] = W[(size_t)(k0 - 1) * cells + c];
+  __syncthreads();
+  for (int k = k0; k < rows; k++) {
+    for (int c = tid; c < cells; c += blockDim.x) u[c] = w[c];
+    __syncthreads();
+    for (int m = 4; m >= 1; m--) {
+      const double cm = h / m;
+      double2 nu[kDualRowCells];
+#pragma unroll
+      for (int q = 0; q < kDualRowCells; q++) {
+        const int c = tid + q * blockDim.x;
+        double ar = 0.0, ai = 0.0;
+        if (c < cells)
+          for (int j = start[c]; j < start[c + 1]; j++) {
+            const double2 a = __ldg(coef + j), z = u[__ldg(idx + j)];
+            ar = fma(a.x, z.x, fma(-a.y, z.y, ar));
+            ai = fma(a.x, z.y, fma(a.y, z.x, ai));
+          }
+        nu[q] = c < cells ? make_double2(fma(cm, ar, w[c].x), fma(cm, ai, w[c].y)) : make_double2(0.0, 0.0);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < kDualRowCells; q++) {
+        const int c = tid + q * blockDim.x;
+        if (c < cells) u[c] = nu[q];
+      }
+      __syncthreads();
+    }
+    for (int c = tid; c < cells; c += blockDim.x) {
+      W[(size_t)k * cells + c] = u[c];
+      w[c] = u[c];
+    }
+    __syncthreads();
+  }
+}
+
 // Extend the dual vectors to `rows` (w_{k+1} = T4(h L^T) w_k in Horner form, FP64) and
-// bring them to the device.
+// bring them to the device.  The chain runs on the device in dual_rows_kernel, on the
+// plan's auxiliary stream, so that it overlaps the slot kernel; ev_join marks its end
+// and the tail kernel waits for it.  Systems with more reduced cells than one CTA holds
+// in registers run the chain on the host.
 static int dual_rows(ScanState &s, int rows, cudaStream_t st) {
   const int cells = s.tail_n * s.n_ado;
+  if (cells <= kDualRowThreads * kDualRowCells && cells > 0) {
+    cudaError_t e = cudaSuccess;
+    const size_t row_bytes = sizeof(double2) * (size_t)cells;
+    if (!s.aux) e = cudaStreamCreateWithFlags(&s.aux, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !s.ev_fork) e = cudaEventCreateWithFlags(&s.ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess && !s.ev_join) e = cudaEventCreateWithFlags(&s.ev_join, cudaEventDisableTiming);
+    // the auxiliary stream starts after everything queued on st (a previous run's tail
+    // kernel may still read rows of W)
+    if (e == cudaSuccess) e = cudaEventRecord(s.ev_fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s.aux, s.ev_fork, 0);
+    if (e == cudaSuccess && (size_t)rows * row_bytes > s.W_cap) {
+      if (s.d_W) cudaFree(s.d_W);
+      s.d_W = nullptr;
+      s.W_cap = 0;
+      s.W_dev_rows = 0;
+      const int cap_rows = std::max(rows, 2 * std::max(s.W_dev_rows, 1));
+      e = cudaMalloc(&s.d_W, (size_t)cap_rows * row_bytes);
+      if (e == cudaSuccess) s.W_cap = (size_t)cap_rows * row_bytes;
+    }
+    if (e == cudaSuccess && s.dual_dirty) { // CSR of L^T and w_0 of the current sample
+      const size_t nnz = s.dual_idx.size();
+      const size_t o_idx = (sizeof(int) * ((size_t)cells + 1) + 255) & ~(size_t)255;
+      const size_t o_coef = (o_idx + sizeof(int) * nnz + 255) & ~(size_t)255;
+      const size_t bytes = o_coef + sizeof(double) * s.dual_coef.size();
+      if (bytes > s.dcsr_cap) {
+        if (s.d_dcsr) cudaFree(s.d_dcsr);
+        s.d_dcsr = nullptr;
+        s.dcsr_cap = 0;
+        e = cudaMalloc(&s.d_dcsr, bytes);
+        if (e == cudaSuccess) s.dcsr_cap = bytes;
+      }
+      s.h_dcsr.assign(bytes, 0);
+      std::memcpy(s.h_dcsr.data(), s.dual_start.data(), sizeof(int) * ((size_t)cells + 1));
+      std::memcpy(s.h_dcsr.data() + o_idx, s.dual_idx.data(), sizeof(int) * nnz);
+      std::memcpy(s.h_dcsr.data() + o_coef, s.dual_coef.data(), sizeof(double) * s.dual_coef.size());
+      s.dcsr_idx = o_idx;
+      s.dcsr_coef = o_coef;
+      if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_dcsr, s.h_dcsr.data(), bytes, cudaMemcpyHostToDevice, s.aux);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_W, s.h_W.data(), row_bytes, cudaMemcpyHostToDevice, s.aux);
+      if (e == cudaSuccess) { s.W_dev_rows = 1; s.dual_dirty = false; }
+    }
+    if (e == cudaSuccess && s.W_dev_rows < 1) { // W reallocated: w_0 again
+      e = cudaMemcpyAsync(s.d_W, s.h_W.data(), row_bytes, cudaMemcpyHostToDevice, s.aux);
+      if (e == cudaSuccess) s.W_dev_rows = 1;
+    }
+    if (e == cudaSuccess && s.W_dev_rows < rows) {
+      const unsigned char *b = (const unsigned char *)s.d_dcsr;
+      const size_t smem = 2 * row_bytes;
+      if (smem > 48 * 1024) e = cudaFuncSetAttribute(dual_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess) {
+        dual_rows_kernel<<<1, kDualRowThreads, smem, s.aux>>>(cells, (const int *)b, (const int *)(b + s.dcsr_idx),
+                                                                (const double2 *)(b + s.dcsr_coef), s.h,
+                                                                (double2 *)s.d_W, s.W_dev_rows, rows);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) { s.W_dev_rows = rows; s.staged_launches++; }
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(s.ev_join, s.aux);
+    if (e == cudaSuccess && s.dual_pos_dirty) {
+      if (!s.d_dualpos) e = cudaMalloc(&s.d_dualpos, sizeof(int) * kTailMax);
+      if (e == cudaSuccess)
+        e = cudaMemcpy(s.d_dualpos, s.dual_pos.data(), sizeof(int) * s.dual_pos.size(), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) s.dual_pos_dirty = false;
+    }
+    if (e != cudaSuccess) { s_err = std::string("dual tail rows: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+    s.dual_on_aux = true;
+    return 0;
+  }
+  s.dual_on_aux = false;
   if (s.W_rows < rows) {
     s.h_W.resize(2 * (size_t)cells * rows);
     std::vector<double> u(2 * (size_t)cells), lu(2 * (size_t)cells);
@@ -2034,16 +2193,11 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   a.jpow = (const double2 *)s.d_jpow;
   a.jpow_stride = s.jpow_elems;
   a.jpow_n = jpow_use; // prepared for this sample by jump_powers above
-  const int grid = std::max(1, std::min(a.n_jobs, s.sl_grid));
-  slot_kernel(s.precision)<<<grid, s.sl_threads, s.sl_smem, st>>>(a);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) { s_err = std::string("staged scan launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
-  s.staged_launches++;
-  s.err_pending = (int *)s.d_flags + n;
+  // the tails' records w_k^T q (scan_tail_dual, G points per CTA): planned here so that
+  // the dual rows they need are formed on the auxiliary stream while the slot kernel runs
+  int kmax = 0;
+  std::vector<DualPoint> dp;
   if (tail_kernel && !tails.empty()) {
-    // records w_k^T q of every tail (scan_tail_dual), G points per CTA
-    int kmax = 0;
-    std::vector<DualPoint> dp;
     dp.reserve(tails.size());
     for (int i : tails) {
       const PtPlan &q = pl[i];
@@ -2059,9 +2213,23 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       kmax = std::max(kmax, d.k0 + (cnt - 1) * s.stride + 1);
       dp.push_back(d);
     }
+  }
+  if (!dp.empty()) {
+    int rc = dual_rows(s, kmax, st);
+    if (rc) return rc;
+  }
+  const int grid = std::max(1, std::min(a.n_jobs, s.sl_grid));
+  slot_kernel(s.precision)<<<grid, s.sl_threads, s.sl_smem, st>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) { s_err = std::string("staged scan launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  s.staged_launches++;
+  s.err_pending = (int *)s.d_flags + n;
+  {
     if (!dp.empty()) {
-      int rc = dual_rows(s, kmax, st);
-      if (rc) return rc;
+      if (s.dual_on_aux) {
+        e = cudaStreamWaitEvent(st, s.ev_join, 0);
+        if (e != cudaSuccess) { s_err = std::string("tail rows wait: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+      }
       e = grow<DualPoint>(s.d_tailpts, s.tailpts_cap, dp.size());
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(s.d_tailpts, dp.data(), sizeof(DualPoint) * dp.size(), cudaMemcpyHostToDevice, st);
@@ -2235,6 +2403,11 @@ void scan_release(ScanState &s) {
   if (s.d_jL) cudaFree(s.d_jL);
   if (s.d_jpow) cudaFree(s.d_jpow);
   if (s.d_jtmp) cudaFree(s.d_jtmp);
+  if (s.d_jdims) cudaFree(s.d_jdims);
+  if (s.d_dcsr) cudaFree(s.d_dcsr);
+  if (s.ev_fork) cudaEventDestroy(s.ev_fork);
+  if (s.ev_join) cudaEventDestroy(s.ev_join);
+  if (s.aux) cudaStreamDestroy(s.aux);
   if (s.d_jobs) cudaFree(s.d_jobs);
   if (s.d_saves) cudaFree(s.d_saves);
   if (s.d_tables) cudaFree(s.d_tables);

@@ -71,6 +71,14 @@ struct ScanState {
   bool dual_pos_dirty = false;
   void *d_W = nullptr, *d_dualpos = nullptr;
   size_t W_cap = 0;
+  // the dual rows on the device: CSR of L^T (start | idx | coef), its upload copy, an
+  // auxiliary stream that overlaps the chain with the slot kernel, fork / join events
+  bool dual_dirty = false, dual_on_aux = false;
+  void *d_dcsr = nullptr;
+  size_t dcsr_cap = 0, dcsr_idx = 0, dcsr_coef = 0;
+  std::vector<unsigned char> h_dcsr;
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // jumps over pulse-free intervals: position blocks (jtab: count, positions per block,
   // first position, matrix offset, positions), dense L0 blocks, powers T0^(2^j) on device
   std::vector<int> jtab, jdims;
@@ -79,7 +87,11 @@ struct ScanState {
   size_t jblocks = 0;
   int jpow_n = 0, jpow_cap = 0;
   bool jL_dirty = false;
-  void *d_jtab = nullptr, *d_jL = nullptr, *d_jpow = nullptr, *d_jtmp = nullptr;
+  void *d_jtab = nullptr, *d_jL = nullptr, *d_jpow = nullptr, *d_jtmp = nullptr, *d_jdims = nullptr;
+  size_t jL_cap = 0, jtab_cap = 0, jmeta_offs = 0; // kept across samples while large enough
+  std::vector<unsigned char> h_jmeta;            // jtab + per-block offsets, as uploaded
+  std::vector<int> h_jdims;                      // block sizes as uploaded
+  int jdims_cap = 0;
   std::vector<heom_scan_point> rb_pts; // points / offsets read back for heom_run_scan_device
   std::vector<long long> rb_off;
   long long staged_launches = 0;
