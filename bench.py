@@ -42,10 +42,12 @@ sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
 METRIC = "2DES propagations/sec, chosen vs plain FP64 on 1 B200 at ≤1e-6 P(t) err"
 UNIT = "propagations/s"
 KEY = os.path.join(ROOT, "tests", "golden", "keys", "c0_dimer.key")
-# dram__bytes_read.sum + dram__bytes_write.sum of the staged scan kernel from one ncu
-# capture of `bench.py --profile-run fp32-bulk` (148 points), per point: the snapshots
-# handed between stages dominate and scale with the number of points.
-DRAM_BYTES_PER_POINT = 239616.0 / 148.0
+# dram__bytes_read.sum + dram__bytes_write.sum of one scan_slots launch of the bench's own
+# 1024-point scan (the second run of a plan, T0 powers cached), from one ncu capture of
+# `bench.py --profile-run fp32-bulk-full` (profiles/scan_slots_dram_dimer_scan.md):
+# 27,223,040 B read (mostly the FP64 jump powers, read cold: ncu and the bench's L2 flush
+# both start the launch with an empty L2) + 5,175,552 B written (snapshots, P records).
+DRAM_BYTES_PER_SCAN = 27223040.0 + 5175552.0
 TEMPLATE = os.path.join(ROOT, "tests", "golden", "keys", "c2_dimer_scan.key-tmpl")
 
 
@@ -480,7 +482,7 @@ def run_ours(a):
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
-                         "traffic": DRAM_BYTES_PER_POINT * n,
+                         "traffic": DRAM_BYTES_PER_SCAN if n == 1024 else None,
                          "executed_component_steps": int(exec_steps), "reference_trajectory_steps": int(traj_steps),
                          "reference_equivalent_tflops": ref_equiv,
                          "note": (f"algorithmic flops = {F:.0f} flop per component-step (4 stages: 16N^3 + 24N^2 "
