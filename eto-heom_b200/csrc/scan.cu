@@ -2058,7 +2058,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     J.first = kNever;
     J.last = 0;
     J.wait_val = 2;
-    J.mode = s.tail_n > 0 ? 1 : 0; // reduced positions when the sample allows it
+    J.mode = 0; // full blocks: with reduced positions the tails run in scan_tail_dual
     set_taus(J, 0, pts[tails[k]]);
     set_taus(J, 1, pts[tails[k]]);
     K.key = 0;
@@ -2188,7 +2188,6 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   a.flags = (int *)s.d_flags;
   a.err = (int *)s.d_flags + n;
   a.wait_ns = wait_ns; // by default far above any legitimate wait
-  a.tail = s.tail_n > 0 ? (const double *)s.d_tail : nullptr;
   a.jtab = (const int *)s.d_jtab;
   a.jpow = (const double2 *)s.d_jpow;
   a.jpow_stride = s.jpow_elems;
@@ -2259,7 +2258,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
   for (const SlotJob &J : jobs) { // propagated component-steps (a reduced step counts its share)
     long long w = 0;
     for (const SlotSpec &z : J.slot) w += std::max(0, std::min(z.stop, J.last) - std::max(z.wake, J.first));
-    s.last_work += J.mode == 1 ? w * s.tail_n / (s.N * s.N) : w - gap_steps(s, tgrid, J, saves, jpow_use);
+    s.last_work += w - gap_steps(s, tgrid, J, saves, jpow_use);
   }
   return 0;
 }

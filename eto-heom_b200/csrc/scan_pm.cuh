@@ -104,12 +104,20 @@ __device__ __forceinline__ void pm_commutator(unsigned mask, const typename V2<T
   T2 zb[NN]; // the whole block: rows l for A z, the thread's rows for z A
 #pragma unroll
   for (int e = 0; e < NN; e++) zb[e] = W[e * SP + blk];
+  // FP32: the operator in registers, so that no shared-memory latency sits inside the
+  // masked products (FP64 keeps reading it from shared memory: registers are short there)
+  constexpr bool kPre = sizeof(T) == 4;
+  T2 av[kPre ? NN : 1];
+  if constexpr (kPre) {
+#pragma unroll
+    for (int e = 0; e < NN; e++) av[e] = A[e];
+  }
 #pragma unroll
   for (int rr = 0; rr < RPT; rr++)
 #pragma unroll
     for (int l = 0; l < NT; l++) {
       if (!(mask & (1u << ((R0 + rr) * NT + l)))) continue;
-      const T2 a = A[(R0 + rr) * NT + l];
+      const T2 a = kPre ? av[kPre ? (R0 + rr) * NT + l : 0] : A[(R0 + rr) * NT + l];
 #pragma unroll
       for (int c = 0; c < NT; c++) { // X[r][c] += a * z[l][c]
         const int e = rr * NT + c;
@@ -125,7 +133,7 @@ __device__ __forceinline__ void pm_commutator(unsigned mask, const typename V2<T
 #pragma unroll
     for (int c = 0; c < NT; c++) {
       if (!(mask & (1u << (l * NT + c)))) continue;
-      const T2 a = A[l * NT + c];
+      const T2 a = kPre ? av[kPre ? l * NT + c : 0] : A[l * NT + c];
 #pragma unroll
       for (int rr = 0; rr < RPT; rr++) { // X[r][c] -= z[r][l] * a
         const int e = rr * NT + c;

@@ -3,35 +3,23 @@
 // The single-pass scan kernel propagates, for every point, the four mixed-difference
 // components R, D2, D3, Q from t_start to the point's end.  Points of a scan share most
 // of that work: R depends only on pulse 1's time, D2 only on pulses 1 and 2, and D3 and
-// Q stay exactly zero until pulse 3's window (see scan_pm.cuh); after the last pulse
-// window D2 and D3 no longer feed Q, and R and Q evolve under the pulse-free operator.
-// The staged scan therefore runs three launches of one kernel over "jobs":
-//   1. per group of points with equal (tau1, tau2): R and D2 from t_start up to the last
-//      member's pulse-3 window, saving both states at each member's window start;
-//   2. per point: R, D2, D3, Q through its pulse-3 window from those states (D3 = Q = 0),
-//      recording P and saving R and Q at the window's end;
-//   3. per four points: D = Q - R of each point from the window's end to the point's
-//      end, recording P = Tr X3 D -- four points per CTA.
-// After the last pulse window R and Q evolve under the same pulse-free operator, so
-// their difference D does too, and P = Tr X3 (Q - R) = Tr X3 D: one trajectory per point
-// instead of two.  D is formed in FP64 at the window's end; its FP32 contraction error
-// scales with |D| rather than with |R| and |Q|.  Stages 1 and 2 perform the single-pass
-// kernel's operations on the same values (bit-identical up to the window's end).
+// Q stay exactly zero until pulse 3's window (see scan_pm.cuh).  The staged scan runs
+// one persistent launch of this kernel over a queue of jobs (scan.cu, staged_run):
+//   1. per (tau1, tau2) group: R and D2 from t_start until the first two pulses are over,
+//      jumping over the pulse-free gap between them, saving D2 (and R where a member
+//      needs it) at the members' window starts or at the group's jump base;
+//   2. jump jobs (mode 2): D2 carried from the base to each member's window start as
+//      T0^(steps) through the block powers of the pulse-free step map;
+//   3. per point: its pulse-3 window (D2 and Q, or R, D2, D3 and Q), recording P and
+//      saving the state at the window's end.
+// The pulse-free tails after the windows run in scan_tail_dual (below) as FP64 dot
+// products with the dual vectors w_k.
 //
-// Reduced tails.  With every pulse off, H (block-diagonal in excitation number) and the
-// bath (site projectors) map each element position of an ADO block to positions coupled
-// by the off-diagonal H only.  P reads the positions where X3 is nonzero; the closure of
-// that set under the off-diagonal H (computed on the host per sample, at most kTailMax
-// positions) evolves on its own.  Tail jobs in reduced mode propagate only those
-// positions: 4 of 16 for the dimer (the (singles, ground) and (doubles, singles) blocks).
-//
-// All three stages run as one persistent launch over a single job queue (stage-1 jobs
-// first, then stage 2, then stage 3).  A job whose inputs come from an earlier job waits
-// on a per-point flag that the producer sets after its snapshot stores are visible.
-// Every producer was dequeued before its consumers, by a CTA that is resident and never
-// waits on a later job, so each wait ends; it is still bounded in time, and a wait that
-// gives up sets an error flag, writes NaN into its outputs and releases its own
-// dependants.
+// A job whose inputs come from an earlier job waits on a per-point flag that the
+// producer sets after its snapshot stores are visible.  Every producer was dequeued
+// before its consumers, by a CTA that is resident and never waits on a later job, so
+// each wait ends; it is still bounded in time, and a wait that gives up sets an error
+// flag, writes NaN into its outputs and releases its own dependants.
 //
 // A job holds up to four "slots" (trajectories).  Slot s has an operator (off-diagonal
 // H plus the pulses in its op mask, with the pulse times of its field set), up to two
@@ -65,7 +53,7 @@ struct SlotJob {
   int first, last;       // steps [first, last)
   int save_begin, save_end;
   int wait[4], wait_val; // start once flags[wait[k]] >= wait_val (-1: no wait)
-  int mode;              // 0: full blocks; 1: the reduced tail positions only
+  int mode;              // 0: slots stepped on full blocks; 2: a jump (see sl_jump)
   double tau[2][3];      // pulse times of the two field sets
   SlotSpec slot[4];
   SlotRec rec[4];
@@ -92,7 +80,6 @@ struct SlotArgs {
   int *flags;            // per-point readiness between stages
   int *err;              // set to 1 when a dependency wait gives up
   unsigned long long wait_ns;
-  const double *tail;    // [n][pos x kTailMax][C: kTailMax x kTailMax complex], see tail_table
   const int *jtab;       // jump blocks: count, positions per block, first position, offset, positions
   const double2 *jpow;   // T0^(2^j) of every block, jpow_stride elements per power
   long long jpow_stride;
@@ -167,133 +154,6 @@ __device__ __forceinline__ void sl_stage(const PmShared &g, int n, int blk, unsi
     const double2 r0v = rho[q * SP + blk];
     const double2 wn = make_double2(fma(cm, k_r, r0v.x), fma(cm, k_i, r0v.y));
     w64[q] = wn;
-    Wn[q * SP + blk] = mk2<T>(wn.x, wn.y);
-    if (last) rho[q * SP + blk] = wn;
-  }
-}
-
-// The same stage for row R0 of the slot's block only (steps with a single live slot: the
-// block's rows are spread over four threads).  Per element the operations and their
-// order are those of sl_stage.
-template <typename T, int NT, int R0>
-__device__ __forceinline__ void sl_stage_row(const PmShared &g, int n, int blk, unsigned am,
-                                             const typename V2<T>::t *A, int sb0, unsigned sm0,
-                                             const typename V2<T>::t *S0, int sb1, unsigned sm1,
-                                             const typename V2<T>::t *S1, const typename V2<T>::t *__restrict__ W,
-                                             typename V2<T>::t *__restrict__ Wn, const double *__restrict__ Hdd,
-                                             double2 *__restrict__ rho, const PmLink<T> *__restrict__ links, int slot,
-                                             double2 dmp, double cm, bool last, double2 (&w64)[NT]) {
-  using T2 = typename V2<T>::t;
-  const int SP = g.SP, nado = g.nado, K = g.K, Km = g.Km;
-  T kr[NT], ki[NT];
-#pragma unroll
-  for (int e = 0; e < NT; e++) { kr[e] = 0; ki[e] = 0; }
-  if (am) pm_commutator<T, NT, 1, R0>(am, A, W, SP, blk, kr, ki);
-#pragma unroll 1
-  for (int k = 0; k < 2; k++) {
-    const int sb = k == 0 ? sb0 : sb1;
-    const unsigned sm = k == 0 ? sm0 : sm1;
-    if (sb >= 0 && sm) pm_commutator<T, NT, 1, R0>(sm, k == 0 ? S0 : S1, W, SP, sb * nado + n, kr, ki);
-  }
-  const T2 *Wc = W + slot * nado;
-  if (K >= 1) pm_links<T, NT, 1, R0, 1>(Wc, SP, nado, K, Km, n, links, kr, ki);
-  if (NT > 2 && K >= 2) pm_links<T, NT, 1, R0, (NT > 2 ? 2 : 1)>(Wc, SP, nado, K, Km, n, links, kr, ki);
-  if (NT > 3 && K >= 3) pm_links<T, NT, 1, R0, (NT > 3 ? 3 : 1)>(Wc, SP, nado, K, Km, n, links, kr, ki);
-#pragma unroll
-  for (int c = 0; c < NT; c++) {
-    const int q = R0 * NT + c;
-    const double gr = dmp.x, gi = dmp.y - Hdd[q];
-    const double2 wv = w64[c];
-    const double k_r = fma(gr, wv.x, fma(-gi, wv.y, (double)kr[c]));
-    const double k_i = fma(gr, wv.y, fma(gi, wv.x, (double)ki[c]));
-    const double2 r0v = rho[q * SP + blk];
-    const double2 wn = make_double2(fma(cm, k_r, r0v.x), fma(cm, k_i, r0v.y));
-    w64[c] = wn;
-    Wn[q * SP + blk] = mk2<T>(wn.x, wn.y);
-    if (last) rho[q * SP + blk] = wn;
-  }
-}
-
-// One Horner stage of the reduced tail: positions tpos[0..ne) of the slot's block.
-template <typename T, int NT>
-__device__ __forceinline__ void sl_stage_tail(const PmShared &g, int n, int blk, int slot, int ne,
-                                              const int *__restrict__ tpos, const unsigned *__restrict__ tmask,
-                                              const typename V2<T>::t *__restrict__ tC,
-                                              const typename V2<T>::t *__restrict__ W,
-                                              typename V2<T>::t *__restrict__ Wn, const double *__restrict__ Hdd,
-                                              double2 *__restrict__ rho, const PmLink<T> *__restrict__ links,
-                                              double2 dmp, double cm, bool last, double2 (&w64)[NT * NT]) {
-  using T2 = typename V2<T>::t;
-  const int SP = g.SP, nado = g.nado, K = g.K, Km = g.Km;
-  T kr[kTailMax], ki[kTailMax];
-  T2 zb[kTailMax];
-#pragma unroll
-  for (int e = 0; e < kTailMax; e++) {
-    kr[e] = 0;
-    ki[e] = 0;
-    zb[e] = e < ne ? W[tpos[e] * SP + blk] : mk2<T>(0.0, 0.0);
-  }
-#pragma unroll
-  for (int e = 0; e < kTailMax; e++) { // X = C z, k = -i X
-    if (e >= ne) break;
-#pragma unroll
-    for (int f = 0; f < kTailMax; f++) {
-      if (!(tmask[e] & (1u << f))) continue;
-      const T2 a = tC[e * kTailMax + f], z = zb[f];
-      ki[e] = fma(-a.x, z.x, ki[e]);
-      ki[e] = fma(a.y, z.y, ki[e]);
-      kr[e] = fma(a.x, z.y, kr[e]);
-      kr[e] = fma(a.y, z.x, kr[e]);
-    }
-  }
-  const T2 *Wc = W + slot * nado;
-#pragma unroll
-  for (int e = 0; e < kTailMax; e++) { // bath links of site levels r (row) and c (column)
-    if (e >= ne) break;
-    const int q = tpos[e], r = q / NT, c = q - r * NT;
-    if (r >= 1 && r <= K)
-      for (int k = 0; k < Km; k++) {
-        const PmLink<T> L = links[((r - 1) + k * K) * nado + n];
-        const unsigned u = (unsigned)L.ud & 0xffffu, d = (unsigned)L.ud >> 16;
-        if (u != 0xffffu && c != r) { // row r: +i x w_u
-          const T2 z = Wc[q * SP + u];
-          kr[e] = fma(-L.x, z.y, kr[e]);
-          ki[e] = fma(L.x, z.x, ki[e]);
-        }
-        if (d != 0xffffu) { // row r: (-b y, a y) w_d; diagonal (-2 b y, 0)
-          const T2 z = Wc[q * SP + d];
-          const T cr = c == r ? -2 * L.by : -L.by, ci = c == r ? (T)0 : L.ay;
-          kr[e] = fma(cr, z.x, fma(-ci, z.y, kr[e]));
-          ki[e] = fma(cr, z.y, fma(ci, z.x, ki[e]));
-        }
-      }
-    if (c >= 1 && c <= K && c != r)
-      for (int k = 0; k < Km; k++) {
-        const PmLink<T> L = links[((c - 1) + k * K) * nado + n];
-        const unsigned u = (unsigned)L.ud & 0xffffu, d = (unsigned)L.ud >> 16;
-        if (u != 0xffffu) { // column c: -i x w_u
-          const T2 z = Wc[q * SP + u];
-          kr[e] = fma(L.x, z.y, kr[e]);
-          ki[e] = fma(-L.x, z.x, ki[e]);
-        }
-        if (d != 0xffffu) { // column c: (-b y, -a y) w_d
-          const T2 z = Wc[q * SP + d];
-          kr[e] = fma(-L.by, z.x, fma(L.ay, z.y, kr[e]));
-          ki[e] = fma(-L.by, z.y, fma(-L.ay, z.x, ki[e]));
-        }
-      }
-  }
-#pragma unroll
-  for (int e = 0; e < kTailMax; e++) {
-    if (e >= ne) break;
-    const int q = tpos[e];
-    const double gr = dmp.x, gi = dmp.y - Hdd[q];
-    const double2 wv = w64[e];
-    const double k_r = fma(gr, wv.x, fma(-gi, wv.y, (double)kr[e]));
-    const double k_i = fma(gr, wv.y, fma(gi, wv.x, (double)ki[e]));
-    const double2 r0v = rho[q * SP + blk];
-    const double2 wn = make_double2(fma(cm, k_r, r0v.x), fma(cm, k_i, r0v.y));
-    w64[e] = wn;
     Wn[q * SP + blk] = mk2<T>(wn.x, wn.y);
     if (last) rho[q * SP + blk] = wn;
   }
@@ -452,10 +312,7 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
   extern __shared__ __align__(16) unsigned char sm[];
   __shared__ double2 s_tr[8];
   __shared__ unsigned s_mask[8];
-  __shared__ int s_tpos[kTailMax], s_tn;
   __shared__ SlotJob s_jobd;
-  __shared__ unsigned s_tmask[kTailMax];
-  __shared__ typename V2<T>::t s_tC[kTailMax * kTailMax];
   __shared__ int s_lo[6], s_cnt[6], s_job, s_ok;
   __shared__ float s_t0;
   const int M = a.M, nado = a.n_ado, K = a.K, Km = a.K_m, wcap = a.wcap;
@@ -503,18 +360,6 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
     Hoff[q] = make_double2(g_Hoff[2 * q], g_Hoff[2 * q + 1]);
   }
   for (int q = tid; q < 3 * NN; q += bs) Xf[q] = make_double2(g_Xs[2 * q], g_Xs[2 * q + 1]);
-  if (tid == 0) s_tn = a.tail ? (int)a.tail[0] : 0;
-  if (tid < kTailMax) {
-    s_tpos[tid] = a.tail ? (int)a.tail[1 + tid] : 0;
-    unsigned m = 0;
-    for (int f = 0; f < kTailMax; f++) {
-      const double cr = a.tail ? a.tail[1 + kTailMax + 2 * (tid * kTailMax + f)] : 0.0;
-      const double ci = a.tail ? a.tail[1 + kTailMax + 2 * (tid * kTailMax + f) + 1] : 0.0;
-      s_tC[tid * kTailMax + f] = mk2<T>(cr, ci);
-      if (cr != 0.0 || ci != 0.0) m |= 1u << f;
-    }
-    s_tmask[tid] = m;
-  }
   const PmShared gsh{SP, nado, M, K, Km};
 
   for (;;) {
@@ -810,53 +655,6 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
           }
 #pragma unroll
       for (int r = 0; r < 4; r++) rcn[r] += rec[r];
-      // a single live full-block slot: its rows are spread over all threads
-      int nlive = 0, ss = 0;
-#pragma unroll
-      for (int z = 0; z < 4; z++)
-        if (i >= J.slot[z].wake && i < J.slot[z].stop) { nlive++; ss = z; }
-      if (nlive == 1 && J.mode == 0 && NT * nado <= bs) {
-        const int r = tid / nado, n2 = tid - r * nado;
-        const bool ok = r < NT;
-        const SlotSpec &sp = J.slot[ss];
-        const int blk2 = ss * nado + (ok ? n2 : 0);
-        const unsigned am2 = s_mask[ss];
-        const int f2 = sp.fset;
-        const bool s0 = sp.src[0] >= 0 && on[3 * f2 + sp.srcq[0]];
-        const bool s1 = sp.src[1] >= 0 && on[3 * f2 + sp.srcq[1]];
-        const int b0 = s0 ? sp.src[0] : -1, b1 = s1 ? sp.src[1] : -1;
-        const unsigned k0 = s0 ? s_mask[4 + 2 * f2 + sp.srcq[0] - 1] : 0u;
-        const unsigned k1 = s1 ? s_mask[4 + 2 * f2 + sp.srcq[1] - 1] : 0u;
-        const T2 *Q0 = Aall + (4 + 2 * f2 + (s0 ? sp.srcq[0] - 1 : 0)) * NN;
-        const T2 *Q1 = Aall + (4 + 2 * f2 + (s1 ? sp.srcq[1] - 1 : 0)) * NN;
-        const double2 dmp2 = ok ? sdamp[n2] : make_double2(0.0, 0.0);
-        double2 wr[NT];
-#pragma unroll
-        for (int c = 0; c < NT; c++) wr[c] = ok ? rho[(r * NT + c) * SP + blk2] : make_double2(0.0, 0.0);
-        for (int m = 4; m >= 1; m--) {
-          const double cm = a.h / m;
-          const T2 *W = w32 + (size_t)buf * EP;
-          T2 *Wn = w32 + (size_t)(buf ^ 1) * EP;
-          if (ok) {
-            if (r == 0)
-              sl_stage_row<T, NT, 0>(gsh, n2, blk2, am2, Aall + ss * NN, b0, k0, Q0, b1, k1, Q1, W, Wn, Hdd, rho,
-                                     links, ss, dmp2, cm, m == 1, wr);
-            else if (r == 1)
-              sl_stage_row<T, NT, (NT > 1 ? 1 : 0)>(gsh, n2, blk2, am2, Aall + ss * NN, b0, k0, Q0, b1, k1, Q1, W,
-                                                    Wn, Hdd, rho, links, ss, dmp2, cm, m == 1, wr);
-            else if (r == 2)
-              sl_stage_row<T, NT, (NT > 2 ? 2 : 0)>(gsh, n2, blk2, am2, Aall + ss * NN, b0, k0, Q0, b1, k1, Q1, W,
-                                                    Wn, Hdd, rho, links, ss, dmp2, cm, m == 1, wr);
-            else
-              sl_stage_row<T, NT, (NT > 3 ? 3 : 0)>(gsh, n2, blk2, am2, Aall + ss * NN, b0, k0, Q0, b1, k1, Q1, W,
-                                                    Wn, Hdd, rho, links, ss, dmp2, cm, m == 1, wr);
-          }
-          buf ^= 1;
-          __syncthreads();
-        }
-        t += a.dt;
-        continue;
-      }
       const bool live = sl >= 0 && i >= my.wake && i < my.stop;
       const int blk = live ? sl * nado + n : 0;
       const unsigned am = live ? s_mask[sl] : 0u;
@@ -870,23 +668,13 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
       const T2 *S0 = Aall + (4 + 2 * f + (son0 ? my.srcq[0] - 1 : 0)) * NN;
       const T2 *S1 = Aall + (4 + 2 * f + (son1 ? my.srcq[1] - 1 : 0)) * NN;
       double2 w64[NN];
-      if (J.mode == 1) { // reduced tail: w64[e] is position s_tpos[e]
 #pragma unroll
-        for (int e = 0; e < NN; e++)
-          w64[e] = (live && e < kTailMax && e < s_tn) ? rho[s_tpos[e < kTailMax ? e : 0] * SP + blk]
-                                                      : make_double2(0.0, 0.0);
-      } else {
-#pragma unroll
-        for (int e = 0; e < NN; e++) w64[e] = live ? rho[e * SP + blk] : make_double2(0.0, 0.0);
-      }
+      for (int e = 0; e < NN; e++) w64[e] = live ? rho[e * SP + blk] : make_double2(0.0, 0.0);
       for (int m = 4; m >= 1; m--) {
         const double cm = a.h / m;
         const T2 *W = w32 + (size_t)buf * EP;
         T2 *Wn = w32 + (size_t)(buf ^ 1) * EP;
-        if (live && J.mode == 1)
-          sl_stage_tail<T, NT>(gsh, n, blk, sl, s_tn, s_tpos, s_tmask, s_tC, W, Wn, Hdd, rho, links, dmp, cm,
-                               m == 1, w64);
-        else if (live)
+        if (live)
           sl_stage<T, NT>(gsh, n, blk, am, Aall + sl * NN, sb0, sm0, S0, sb1, sm1, S1, W, Wn, Hdd, rho, links, sl,
                           dmp, cm, m == 1, w64);
         buf ^= 1;
