@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -192,7 +193,30 @@ __global__ void __launch_bounds__(256) sg_ops(SgArgs a, int step_local, const in
 // (r, c0..c0+3) of one ADO block from shared memory, over the nonzero rows/columns of
 // each operator only.  Phase 2: element-per-thread (coalesced) bath couplings, FP64
 // diagonal and damping, and the Horner update.
-template <typename T>
+// Phase-1 products for precision studies of a tensor-core commutator (FP32 state copies):
+// TF = 0: FP32 products; TF = 1: both factors rounded to TF32 (cvt.rna.tf32.f32) first,
+// the product exact in FP32 and accumulated in FP32, as one TF32 tensor-core MMA does;
+// TF = 3: the 3xTF32 split a = a_hi + a_lo, z = z_hi + z_lo, accumulating
+// a_lo z_hi + a_hi z_lo + a_hi z_hi (a_lo z_lo dropped).
+__device__ __forceinline__ float tf32_rna(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+template <typename T, int TF> __device__ __forceinline__ T sg_mac(T acc, T a, T z) {
+  if constexpr (TF == 0 || sizeof(T) != 4) {
+    return fma(a, z, acc);
+  } else if constexpr (TF == 1) {
+    return fma(tf32_rna(a), tf32_rna(z), acc);
+  } else {
+    const float ah = tf32_rna(a), al = tf32_rna(a - ah), zh = tf32_rna(z), zl = tf32_rna(z - zh);
+    acc = fma(al, zh, acc);
+    acc = fma(ah, zl, acc);
+    return fma(ah, zh, acc);
+  }
+}
+
+template <typename T, int TF = 0>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) sg_stage(SgArgs a, int m, int step_local, const int *__restrict__ base) {
   using T2 = typename Vec2<T>::t;
   const int p = blockIdx.z, cq = blockIdx.y;
@@ -308,10 +332,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) sg_stage(SgArgs a
         Quad<T>::load(Wb + l * S + c0, z1);
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-          xr[e] = fma(a1.x, z1[e].x, xr[e]);
-          xr[e] = fma(-a1.y, z1[e].y, xr[e]);
-          xi[e] = fma(a1.x, z1[e].y, xi[e]);
-          xi[e] = fma(a1.y, z1[e].x, xi[e]);
+          xr[e] = sg_mac<T, TF>(xr[e], a1.x, z1[e].x);
+          xr[e] = sg_mac<T, TF>(xr[e], -a1.y, z1[e].y);
+          xi[e] = sg_mac<T, TF>(xi[e], a1.x, z1[e].y);
+          xi[e] = sg_mac<T, TF>(xi[e], a1.y, z1[e].x);
         }
       }
       // - W A: the nonzero entries of columns c0..c0+3 of A
@@ -327,10 +351,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) sg_stage(SgArgs a
         Quad<T>::load(Ab + l * S + c0, a2);
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-          xr[e] = fma(-z2.x, a2[e].x, xr[e]);
-          xr[e] = fma(z2.y, a2[e].y, xr[e]);
-          xi[e] = fma(-z2.x, a2[e].y, xi[e]);
-          xi[e] = fma(-z2.y, a2[e].x, xi[e]);
+          xr[e] = sg_mac<T, TF>(xr[e], -z2.x, a2[e].x);
+          xr[e] = sg_mac<T, TF>(xr[e], z2.y, a2[e].y);
+          xi[e] = sg_mac<T, TF>(xi[e], -z2.x, a2[e].y);
+          xi[e] = sg_mac<T, TF>(xi[e], -z2.y, a2[e].x);
         }
       }
     }
@@ -404,7 +428,6 @@ __global__ void sg_bump(int *base, int by) { *base += by; }
 // ------------------------------------------------------------------ host
 namespace {
 
-template <class T> void *stage_fn() { return (void *)sg_stage<T>; }
 
 int fail(int code, const std::string &m) {
   sg_err = m;
@@ -442,6 +465,15 @@ int sg_init(SgState &s, const heom::Problem &p, int precision, cudaStream_t st) 
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (NN > 1024 || s.smem > (size_t)max_smem) return fail(HEOM_ERR_UNSUPPORTED, "system too large for the staged path");
   SGCK(cudaFuncSetAttribute(sg_stage<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem));
+  // precision study of a tensor-core commutator: HEOM_SG_CONTRACTION=tf32 | tf32x3 rounds
+  // the FP32-bulk phase-1 products as TF32 MMAs would (see sg_mac)
+  if (const char *v = std::getenv("HEOM_SG_CONTRACTION")) {
+    if (!std::strcmp(v, "tf32")) s.tf = 1;
+    else if (!std::strcmp(v, "tf32x3")) s.tf = 3;
+    else if (std::strcmp(v, "fp32")) return fail(HEOM_ERR_ARG, std::string("HEOM_SG_CONTRACTION: unknown value ") + v);
+  }
+  SGCK(cudaFuncSetAttribute(sg_stage<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem));
+  SGCK(cudaFuncSetAttribute(sg_stage<float, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem));
   SGCK(cudaFuncSetAttribute(sg_stage<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem));
   const int ops_smem = (int)(3 * (size_t)s.N * sg_stride(s.N) * tsz);
   SGCK(cudaFuncSetAttribute(sg_ops<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, ops_smem));
@@ -633,6 +665,8 @@ int sg_run(SgState &s, const heom::Problem &p, int C, const int mask[3], const h
     else sg_ops<float><<<ogrid, 256, osmem, st>>>(a, k, s.d_base);
     for (int m = 4; m >= 1; m--) {
       if (d) sg_stage<double><<<grid, s.threads, s.smem, st>>>(a, m, k, s.d_base);
+      else if (s.tf == 1) sg_stage<float, 1><<<grid, s.threads, s.smem, st>>>(a, m, k, s.d_base);
+      else if (s.tf == 3) sg_stage<float, 3><<<grid, s.threads, s.smem, st>>>(a, m, k, s.d_base);
       else sg_stage<float><<<grid, s.threads, s.smem, st>>>(a, m, k, s.d_base);
     }
   }

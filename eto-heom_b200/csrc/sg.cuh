@@ -21,6 +21,7 @@ struct SgState {
   int precision = HEOM_FP32_BULK;
   int N = 0, n_ado = 0, M = 0, K = 0, K_m = 0;
   int apc = 1, threads = 32;          // ADOs per CTA, threads per CTA
+  int tf = 0;                         // FP32-bulk phase-1 products: 0 FP32, 1 TF32, 3 3xTF32 (study)
   size_t smem = 0;
   // problem tables (device)
   void *d_tab = nullptr;              // Hd, Hoff, Xs, X3, damp, alpha, xc, yc, up, dn
