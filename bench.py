@@ -355,7 +355,7 @@ def run_ours(a):
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = plan.launches
-    times = []
+    times, host_ms = [], []
     with Clocks(local) as clk:
         for _ in range(a.steps):
             flush.fill_(1.0)
@@ -363,7 +363,9 @@ def run_ours(a):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            one_scan()
+            h0 = time.perf_counter()
+            one_scan()  # returns once queued: the point read-back, the host planning, the launches
+            host_ms.append(1e3 * (time.perf_counter() - h0))
             torch.cuda.synchronize()
             e1.record(stream)
             torch.cuda.synchronize()
@@ -407,6 +409,11 @@ def run_ours(a):
     achieved = F * exec_steps / (ms / 1e3) / 1e12
     ref_equiv = F * traj_steps / (ms / 1e3) / 1e12
     peak = fp32_peak_tflops(heom, local)
+    # Mixed-pipe bound of the FP32-bulk kernel: the 24 N^2 per-ADO stage work (damping,
+    # site-energy diagonal, Horner update) runs in FP64, the rest in FP32.
+    peak64 = max(heom.fma_peak_tflops(local, fp64=True) for _ in range(3))
+    F64 = 4.0 * inf.n_ado * 24 * inf.sys_size ** 2
+    t_bound = exec_steps * ((F - F64) / (peak * 1e12) + F64 / (peak64 * 1e12))
 
     out = None
     if rank == 0:
@@ -480,8 +487,11 @@ def run_ours(a):
                     "d2h_bytes_per_step": int(16 * tot)},
             "e2e_cold": e2e_cold,
             "gpu_launches": int(launches),
+            "host_ms_per_step": float(np.median(host_ms)),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
+                         "frac_mixed": t_bound / (ms / 1e3),
+                         "peak_fp64": peak64,
                          "traffic": DRAM_BYTES_PER_SCAN if n == 1024 else None,
                          "executed_component_steps": int(exec_steps), "reference_trajectory_steps": int(traj_steps),
                          "reference_equivalent_tflops": ref_equiv,
@@ -489,7 +499,10 @@ def run_ours(a):
                                   "per ADO, 16N per link) x the component-steps the staged scan propagates; "
                                   "reference_equivalent counts the reference's 3 trajectories x all steps; "
                                   "peak = FP32 FMA throughput measured in this run by the library's "
-                                  "FMA-loop kernel (MEASURED_PEAKS.json holds only HBM and bf16 tensor peaks)")},
+                                  "FMA-loop kernel (MEASURED_PEAKS.json holds only HBM and bf16 tensor peaks); "
+                                  "frac_mixed = the time the FP32 work (16N^3 + links) needs at the FP32 peak "
+                                  "plus the time the FP64 work (24N^2 per ADO and stage) needs at the measured "
+                                  "FP64 FMA peak, over the measured time")},
             "accuracy": {"fp32_bulk_vs_fp64_max_rel_err": float(max(errs)),
                          "fp32_bulk_vs_fp64_median_rel_err": float(np.median(errs)), "points_checked": n},
             "plain_fp64": {"value": plain_val, "unit": UNIT, "sample": f"{len(sample_idx)} points, one at a time, "
