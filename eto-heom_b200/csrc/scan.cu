@@ -894,7 +894,8 @@ cudaError_t scan_enqueue(const ScanState &s, const heom_scan_point *d_pts, int n
 
 // Reduced-tail table of the current sample: the positions P reads (X3[l][j] != 0 reads
 // element (j, l)), closed under the off-diagonal H, and the commutator with H restricted
-// to them (see scan_slots.cuh).  n = 0 when the closure exceeds kTailMax positions.
+// to them.  The positions define the cells of the dual tails (dual_operator).  n = 0 when
+// the closure exceeds kTailMax positions.
 static void tail_table(const std::vector<double> &sys, int N, std::vector<double> &tab) {
   const int NN = N * N;
   const double *Hoff = sys.data() + N, *X3 = Hoff + 2 * NN + 6 * NN;
@@ -942,12 +943,10 @@ int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
   if (!s.supported) return 0;
   std::vector<double> sys;
   scan_system_host(p, sys);
-  if (s.staged && s.d_tail) {
+  if (s.staged) { // the reduced tail positions of this sample and their dual operator
     std::vector<double> tab;
     tail_table(sys, s.N, tab);
     s.tail_n = (int)tab[0];
-    cudaError_t e = cudaMemcpyAsync(s.d_tail, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) { s_err = std::string("tail table upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
     if (s.tail_n > 0) dual_operator(s, sys, tab);
   }
   if (s.staged) jump_operator(s, sys);
@@ -2298,7 +2297,6 @@ int scan_init(ScanState &s, const heom::Problem &p, int precision, int max_point
   if (e == cudaSuccess) e = cudaMalloc(&s.d_counter, sizeof(int) * 4);
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_pts, sizeof(heom_scan_point) * max_points);
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_offsets, sizeof(long long) * max_points);
-  if (e == cudaSuccess && s.staged) e = cudaMalloc(&s.d_tail, sizeof(double) * tail_doubles());
   if (e != cudaSuccess) { s_err = std::string("scan buffers: ") + cudaGetErrorString(e); return HEOM_ERR_NOMEM; }
   s.supported = true;
   int rc = scan_upload_system(s, p, st);
@@ -2394,7 +2392,6 @@ void scan_release(ScanState &s) {
   if (s.gexec) cudaGraphExecDestroy(s.gexec);
   if (s.d_snap) cudaFree(s.d_snap);
   if (s.d_flags) cudaFree(s.d_flags);
-  if (s.d_tail) cudaFree(s.d_tail);
   if (s.d_tailpts) cudaFree(s.d_tailpts);
   if (s.d_W) cudaFree(s.d_W);
   if (s.d_dualpos) cudaFree(s.d_dualpos);

@@ -58,7 +58,6 @@ struct ScanState {
   bool inject_unmet = false;     // one consumer job waits for a flag value never set
   long long last_work = 0;       // component-steps propagated by the last staged run
   std::vector<float> t_grid;     // float time of each step (t_start + dt accumulated)
-  void *d_tail = nullptr;        // reduced-tail table of the current sample
   int tail_n = 0;                // its positions (0: tails run on full blocks)
   void *d_tailpts = nullptr;     // the tail kernel's points
   size_t tailpts_cap = 0;

@@ -688,7 +688,7 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
 // ------------------------------------------------------------------ tail kernel
 // The pulse-free tails of a staged scan, after the slot kernel.  Once every pulse is off
 // the step map is one fixed matrix T = sum_{j<=4} (hL)^j / j! (L: the pulse-free HEOM
-// operator on the reduced positions, see tail_doubles), the same for every point, so
+// operator on the reduced positions of the tail table), the same for every point, so
 // the tail records of a point with state q at its window end s3 are
 //   P(s3 + k) = x3^T T^k q = w_k^T q,   w_k = (T^T)^k x3,
 // x3 the readout (Tr X3 . on ADO 0).  The host propagates the dual vectors w_k once per

@@ -138,3 +138,25 @@ def test_staged_scan_matches_single_pass(setup, precision, tol):
     torch.cuda.synchronize()
     Pd = d_P.cpu().numpy().view(np.complex128)
     assert np.array_equal(Pd, a.P[:lay[3]])
+
+
+@pytest.mark.parametrize("precision", ["fp32-bulk", "fp64"])
+def test_scan_edge_cases(setup, precision):
+    """An empty scan, and a staged scan mixing ordinary points with points that record
+    nothing (end before pulse 3) and a point that ends inside pulse 3's window: the
+    empty points get no output and leave the others unchanged."""
+    heom, prob = setup
+    plan = heom.Plan(prob, precision, max_points=16)
+    empty = plan.run_scan(heom.make_points([]))
+    assert len(empty.P) == 0
+    base = scan_geometry()[:4]
+    odd = [(50.0, 100.0, 300.0, 250.0),   # ends before pulse 3: no record
+           (50.0, 60.0, 200.0, 210.0),    # ends inside pulse 3's window
+           (60.0, 50.0, 400.0, 120.0)]    # ends before pulse 2
+    mixed = base[:2] + odd + base[2:]
+    r = plan.run_scan(heom.make_points(mixed))
+    alone = plan.run_scan(heom.make_points(base))
+    assert r.counts[2] == 0 and r.counts[4] == 0 and r.counts[3] > 0
+    for j, i in enumerate([0, 1, 5, 6]):
+        assert rel_err(r.point(i), alone.point(j)) <= (1e-6 if precision == "fp32-bulk" else 1e-11)
+    assert np.isfinite(r.P).all()
