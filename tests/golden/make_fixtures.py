@@ -236,7 +236,8 @@ def parse_driver_output(text):
 DYNAMICS = ["d_dimer.key", "d_trimer.key"]
 GOLDEN = ["c0_dimer_short.key", "c0_dimer.key", "c4_trimer_short.key", "t_disorder.key",
           "t_ref_example.key", "t_strong.key", "c1_fmo_short.key",
-          "c1_fmo_300fs.key"]   # the last one is ~12 min of CPU (dense N = 29 zgemm)
+          "c1_fmo_300fs.key",   # ~12 min of CPU (dense N = 29 zgemm)
+          "c1_fmo.key"]         # ~2 h 20 min of CPU (4001 steps)
 
 
 # The delay scan of the heom_scan driver test (gen_2d_data.sh parameters).

@@ -21,6 +21,18 @@ SMEM_KEYS = ["c0_dimer_short.key", "t_disorder.key", "t_ref_example.key", "t_str
 STAGED_KEYS = ["c4_trimer_short.key", "c1_fmo_short.key", "c1_fmo_300fs.key"]
 
 
+def test_exact_full_fmo_bit_identical():
+    """Config 1 at its stated length: the FMO aggregate (N = 29, 680 ADOs) for 4001 RK4
+    steps (0-2000 fs, 3501 records), identical bits to the reference build run here
+    (2 h 19 min of CPU for the reference's dense zgemm form)."""
+    heom = load_pkg()
+    traj_ref, comb_ref = golden("c1_fmo.key")
+    _, comb, traj = run_key(heom, "c1_fmo.key")
+    assert traj.shape == traj_ref.shape == (1, 3, 3501)
+    assert np.array_equal(traj, traj_ref), f"max rel err {rel_err(traj, traj_ref):.3e}"
+    assert np.array_equal(comb, comb_ref), f"max rel err {rel_err(comb, comb_ref):.3e}"
+
+
 def run_key(heom, name, precision="fp64-exact"):
     prob = heom.Problem.from_key(key(name))
     info = prob.info
