@@ -941,6 +941,7 @@ static void jump_operator(ScanState &s, const std::vector<double> &sys);
 
 int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
   if (!s.supported) return 0;
+  s.sample_gen++; // a planned staged scan is not replayed across samples
   std::vector<double> sys;
   scan_system_host(p, sys);
   if (s.staged) { // the reduced tail positions of this sample and their dual operator
@@ -1790,8 +1791,9 @@ static long long gap_steps(const ScanState &s, const TimeGrid &g, const SlotJob 
   return skipped;
 }
 
-int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, const long long *offsets,
-               cudaStream_t st) {
+static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, const long long *offsets,
+                           cudaStream_t st) {
+  s.rp.valid = false;
   const int NN = s.N * s.N;
   const size_t snap_elems = (size_t)NN * s.n_ado; // double2 per state
   std::vector<PtPlan> pl(n);
@@ -2147,6 +2149,7 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     }
     if (bad) { s_err = std::string("staged scan plan check failed: ") + bad; return HEOM_ERR_CUDA; }
   }
+  const bool injected = s.inject_unmet || s.inject_wait_ns; // the job table then differs: never replayed
   const unsigned long long wait_ns = s.inject_wait_ns ? s.inject_wait_ns : 30ull * 1000 * 1000 * 1000;
   if (s.inject_unmet) // test hook: the first consumer waits for a flag value no producer sets
     for (SlotJob &J : jobs)
@@ -2251,6 +2254,10 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
       }
       if (e != cudaSuccess) { s_err = std::string("tail launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
       s.staged_launches++;
+      static_assert(sizeof(DualArgs) <= sizeof(s.rp.da), "replay buffer");
+      std::memcpy(s.rp.da, &da, sizeof da);
+      s.rp.tail_grid = (int)((dp.size() + kDualG - 1) / kDualG);
+      s.rp.tail_smem = smem;
     }
   }
   s.last_work = 0;
@@ -2259,7 +2266,82 @@ int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, con
     for (const SlotSpec &z : J.slot) w += std::max(0, std::min(z.stop, J.last) - std::max(z.wake, J.first));
     s.last_work += w - gap_steps(s, tgrid, J, saves, jpow_use);
   }
+  // what a repeat of this scan needs to run again without planning (staged_run)
+  if (!injected) {
+    static_assert(sizeof(SlotArgs) <= sizeof(s.rp.a), "replay buffer");
+    std::memcpy(s.rp.a, &a, sizeof a);
+    s.rp.grid = grid;
+    s.rp.nflags = (size_t)n + 1 + groups.size();
+    s.rp.jpow_use = jpow_use;
+    s.rp.kmax = kmax;
+    s.rp.tails = !dp.empty();
+    s.rp.work = s.last_work;
+    s.rp.n = n;
+    s.rp.d_P = d_P;
+    s.rp.snap = s.d_snap;
+    s.rp.sample = s.sample_gen;
+    s.rp.pts.assign(pts, pts + n);
+    s.rp.offsets.assign(offsets, offsets + n);
+    s.rp.valid = true;
+  }
   return 0;
+}
+
+// A repeat of the last planned scan (same points, offsets, output buffer and sample): the
+// job tables, saves and tail points on the device are still those of that plan, so only
+// the per-run state is reset before the two launches.
+static int staged_replay(ScanState &s, cudaStream_t st) {
+  const ScanState::Replay &r = s.rp;
+  cudaError_t e = cudaMemsetAsync(s.d_counter, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.d_flags, 0, sizeof(int) * r.nflags, st);
+  if (e != cudaSuccess) { s_err = std::string("staged scan reset: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  if (r.jpow_use > 0) { // prepared for this sample already: no work unless it was dropped
+    const int rc = jump_powers(s, r.jpow_use, st);
+    if (rc) return rc;
+  }
+  if (r.tails) {
+    const int rc = dual_rows(s, r.kmax, st);
+    if (rc) return rc;
+  }
+  SlotArgs a;
+  std::memcpy(&a, r.a, sizeof a);
+  a.jtab = (const int *)s.d_jtab;
+  a.jpow = (const double2 *)s.d_jpow;
+  slot_kernel(s.precision)<<<r.grid, s.sl_threads, s.sl_smem, st>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) { s_err = std::string("staged scan launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  s.staged_launches++;
+  s.err_pending = a.err;
+  if (r.tails) {
+    if (s.dual_on_aux) {
+      e = cudaStreamWaitEvent(st, s.ev_join, 0);
+      if (e != cudaSuccess) { s_err = std::string("tail rows wait: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+    }
+    DualArgs da;
+    std::memcpy(&da, r.da, sizeof da);
+    da.W = (const double2 *)s.d_W;
+    da.W_rows = s.W_dev_rows;
+    scan_tail_dual<<<r.tail_grid, kDualThreads, r.tail_smem, st>>>(da);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { s_err = std::string("tail launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+    s.staged_launches++;
+  }
+  s.last_work = r.work;
+  return 0;
+}
+
+// Staged scan: plan the jobs on the host and launch, or replay the last plan when the
+// scan repeats it exactly (a bench loop, or the samples of a disorder average, which
+// differ only in the system matrices: those change the sample counter and force a plan).
+int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, const long long *offsets,
+               cudaStream_t st) {
+  const ScanState::Replay &r = s.rp;
+  if (r.valid && !s.inject_unmet && !s.inject_wait_ns && r.n == n && r.d_P == d_P && r.snap == s.d_snap &&
+      r.sample == s.sample_gen && n > 0 &&
+      std::memcmp(r.pts.data(), pts, sizeof(heom_scan_point) * n) == 0 &&
+      std::memcmp(r.offsets.data(), offsets, sizeof(long long) * n) == 0)
+    return staged_replay(s, st);
+  return staged_plan_run(s, pts, n, d_P, offsets, st);
 }
 
 // Status of the last staged run once the stream has drained: a dependency wait that gave

@@ -94,6 +94,21 @@ struct ScanState {
   std::vector<heom_scan_point> rb_pts; // points / offsets read back for heom_run_scan_device
   std::vector<long long> rb_off;
   long long staged_launches = 0;
+  // replay of the last planned staged scan (staged_run): valid while the points, offsets,
+  // output buffer, snapshot buffer and sample are unchanged; the kernel arguments are
+  // kept as bytes (SlotArgs, DualArgs of scan_slots.cuh)
+  long long sample_gen = 0;      // bumped by every system upload
+  struct Replay {
+    bool valid = false, tails = false;
+    int n = 0, grid = 0, jpow_use = 0, kmax = 0, tail_grid = 0;
+    size_t nflags = 0, tail_smem = 0;
+    long long work = 0, sample = -1;
+    const void *d_P = nullptr, *snap = nullptr;
+    std::vector<heom_scan_point> pts;
+    std::vector<long long> offsets;
+    alignas(16) unsigned char a[512];
+    alignas(16) unsigned char da[128];
+  } rp;
   // graph cache for heom_run_scan_device
   cudaGraphExec_t gexec = nullptr;
   const void *g_key[4] = {nullptr, nullptr, nullptr, nullptr};

@@ -160,3 +160,27 @@ def test_scan_edge_cases(setup, precision):
     for j, i in enumerate([0, 1, 5, 6]):
         assert rel_err(r.point(i), alone.point(j)) <= (1e-6 if precision == "fp32-bulk" else 1e-11)
     assert np.isfinite(r.P).all()
+
+
+def test_staged_replay_matches_planned_run():
+    """A repeated staged scan skips the host planning and replays the last plan; a new
+    sample (plan.update) must plan again.  Both give the bits of a freshly planned run."""
+    heom = load_pkg()
+    rows = scan_geometry()
+    pts = heom.make_points(rows)
+    pa = heom.Problem.from_key(key("c0_dimer.key"))
+    pa.prepare_sample()
+    plan = heom.Plan(pa, "fp32-bulk", max_points=len(rows))
+    first = plan.run_scan(pts)
+    work = plan.scan_work
+    again = plan.run_scan(pts)                    # replayed
+    assert np.array_equal(first.P, again.P) and plan.scan_work == work
+    pa.prepare_sample()
+    plan.update()
+    second = plan.run_scan(pts)                   # planned again for the new sample
+    pb = heom.Problem.from_key(key("c0_dimer.key"))
+    pb.prepare_sample()
+    pb.prepare_sample()
+    fresh = heom.Plan(pb, "fp32-bulk", max_points=len(rows)).run_scan(pts)
+    assert np.array_equal(second.P, fresh.P)
+    assert not np.array_equal(second.P, first.P)
