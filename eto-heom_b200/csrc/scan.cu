@@ -941,7 +941,6 @@ static void jump_operator(ScanState &s, const std::vector<double> &sys);
 
 int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
   if (!s.supported) return 0;
-  s.sample_gen++; // a planned staged scan is not replayed across samples
   std::vector<double> sys;
   scan_system_host(p, sys);
   if (s.staged) { // the reduced tail positions of this sample and their dual operator
@@ -968,6 +967,11 @@ int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st) {
            X3[2 * j * s.N + 1] == 0.0;
     s.r_row0 = r0;
   }
+  // what the staged planner reads of a sample: a plan is replayed for a new sample only if
+  // these agree (disorder and orientation draws change values, not this structure)
+  s.structure.assign({s.rstat ? 1 : 0, s.r_row0 ? 1 : 0, s.tail_n});
+  s.structure.insert(s.structure.end(), s.dual_pos.begin(), s.dual_pos.end());
+  s.structure.insert(s.structure.end(), s.jtab.begin(), s.jtab.end());
   cudaError_t e = cudaMemcpyAsync(s.d_sys, sys.data(), sizeof(double) * sys.size(), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) { s_err = std::string("scan system upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
@@ -2279,7 +2283,7 @@ static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, doub
     s.rp.n = n;
     s.rp.d_P = d_P;
     s.rp.snap = s.d_snap;
-    s.rp.sample = s.sample_gen;
+    s.rp.structure = s.structure;
     s.rp.pts.assign(pts, pts + n);
     s.rp.offsets.assign(offsets, offsets + n);
     s.rp.valid = true;
@@ -2331,13 +2335,14 @@ static int staged_replay(ScanState &s, cudaStream_t st) {
 }
 
 // Staged scan: plan the jobs on the host and launch, or replay the last plan when the
-// scan repeats it exactly (a bench loop, or the samples of a disorder average, which
-// differ only in the system matrices: those change the sample counter and force a plan).
+// scan repeats it: the same points, offsets and buffers, and a sample of the same
+// structure (a bench loop, or the samples of a disorder average).  A new sample's T0
+// powers and dual rows are formed by the replay as by a planned run.
 int staged_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, const long long *offsets,
                cudaStream_t st) {
   const ScanState::Replay &r = s.rp;
   if (r.valid && !s.inject_unmet && !s.inject_wait_ns && r.n == n && r.d_P == d_P && r.snap == s.d_snap &&
-      r.sample == s.sample_gen && n > 0 &&
+      r.structure == s.structure && n > 0 &&
       std::memcmp(r.pts.data(), pts, sizeof(heom_scan_point) * n) == 0 &&
       std::memcmp(r.offsets.data(), offsets, sizeof(long long) * n) == 0)
     return staged_replay(s, st);

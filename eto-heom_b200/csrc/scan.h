@@ -95,14 +95,15 @@ struct ScanState {
   std::vector<long long> rb_off;
   long long staged_launches = 0;
   // replay of the last planned staged scan (staged_run): valid while the points, offsets,
-  // output buffer, snapshot buffer and sample are unchanged; the kernel arguments are
+  // output buffer, snapshot buffer and sample structure are unchanged; the kernel arguments are
   // kept as bytes (SlotArgs, DualArgs of scan_slots.cuh)
-  long long sample_gen = 0;      // bumped by every system upload
+  std::vector<int> structure;    // what the planner reads of the sample (scan_upload_system)
   struct Replay {
     bool valid = false, tails = false;
     int n = 0, grid = 0, jpow_use = 0, kmax = 0, tail_grid = 0;
     size_t nflags = 0, tail_smem = 0;
-    long long work = 0, sample = -1;
+    long long work = 0;
+    std::vector<int> structure;
     const void *d_P = nullptr, *snap = nullptr;
     std::vector<heom_scan_point> pts;
     std::vector<long long> offsets;

@@ -163,8 +163,9 @@ def test_scan_edge_cases(setup, precision):
 
 
 def test_staged_replay_matches_planned_run():
-    """A repeated staged scan skips the host planning and replays the last plan; a new
-    sample (plan.update) must plan again.  Both give the bits of a freshly planned run."""
+    """A repeated staged scan skips the host planning and replays the last plan, also for
+    a new sample of the same structure (plan.update), whose T0 powers and dual rows are
+    formed again.  Both give the bits of a freshly planned run."""
     heom = load_pkg()
     rows = scan_geometry()
     pts = heom.make_points(rows)
@@ -177,7 +178,7 @@ def test_staged_replay_matches_planned_run():
     assert np.array_equal(first.P, again.P) and plan.scan_work == work
     pa.prepare_sample()
     plan.update()
-    second = plan.run_scan(pts)                   # planned again for the new sample
+    second = plan.run_scan(pts)                   # replayed on the new sample
     pb = heom.Problem.from_key(key("c0_dimer.key"))
     pb.prepare_sample()
     pb.prepare_sample()
