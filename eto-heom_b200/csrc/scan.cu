@@ -1300,7 +1300,7 @@ void staged_prepare(ScanState &s) {
   s.sl_wcap = pm_window_cap(s.taup, s.dt);
   if (sl_smem_bytes<4>(tsz, s.n_ado, s.M, s.sl_wcap) + 1024 > (size_t)max_smem) s.sl_wcap = 0;
   s.sl_smem = sl_smem_bytes<4>(tsz, s.n_ado, s.M, s.sl_wcap);
-  s.sl_threads = (4 * s.n_ado + 31) / 32 * 32;
+  s.sl_threads = std::max(64, (4 * s.n_ado + 31) / 32 * 32); // warp 1 forms the traces
   if (s.sl_smem + 1024 > (size_t)max_smem || s.sl_threads > kSlotThreads || s.n_ado >= 0xffff) return;
   SlotFn f = slot_kernel(s.precision);
   if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.sl_smem) != cudaSuccess) {

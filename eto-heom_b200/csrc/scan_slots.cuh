@@ -566,13 +566,10 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
       const bool rebuild = anyon || rec[0] || rec[1] || rec[2] || rec[3] || !fieldfree;
       fieldfree = !anyon;
       if (rebuild && tid < 32) {
-        // warp 0: the slots' operators, the pulse-2/3 operators of both field sets, their
-        // nonzero masks, and the traces of the recorders' slots (one element per lane)
+        // warp 0: the slots' operators, the pulse-2/3 operators of both field sets and their
+        // nonzero masks (one element per lane); warp 1 forms the recorders' traces meanwhile
         const int q = tid;
         bool nz[8] = {false, false, false, false, false, false, false, false};
-        double2 c4[8];
-#pragma unroll
-        for (int c = 0; c < 8; c++) c4[c] = make_double2(0.0, 0.0);
         if (q < NN) {
           double vr[6], vi[6];
 #pragma unroll
@@ -607,6 +604,19 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
               Aall[(4 + 2 * f + k) * NN + q] = v;
               nz[4 + 2 * f + k] = v.x != (T)0 || v.y != (T)0;
             }
+        }
+#pragma unroll
+        for (int s = 0; s < 8; s++) {
+          const unsigned b = __ballot_sync(0xffffffffu, nz[s]);
+          if (q == 0) s_mask[s] = b;
+        }
+      } else if (rebuild && tid < 64 && (rec[0] || rec[1] || rec[2] || rec[3])) {
+        // warp 1: Tr X3 of the recorders' slots at the step's start (one element per lane)
+        const int q = tid - 32;
+        double2 c4[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) c4[c] = make_double2(0.0, 0.0);
+        if (q < NN) {
 #pragma unroll
           for (int r = 0; r < 4; r++)
             if (rec[r]) {
@@ -620,11 +630,6 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
                 c4[2 * r + 1] = make_double2(u.x * x.x - u.y * x.y, u.x * x.y + u.y * x.x);
               }
             }
-        }
-#pragma unroll
-        for (int s = 0; s < 8; s++) {
-          const unsigned b = __ballot_sync(0xffffffffu, nz[s]);
-          if (q == 0) s_mask[s] = b;
         }
 #pragma unroll
         for (int r = 0; r < 4; r++)
