@@ -297,7 +297,7 @@ class Plan:
 
     def run_scan(self, points: np.ndarray, layout=None) -> ScanResult:
         pts, off, cnt, tot = layout if layout is not None else self.scan_layout(points)
-        P = np.zeros(max(tot, 1), dtype=np.complex128)
+        P = np.empty(max(tot, 1), dtype=np.complex128)  # every value is written by the call
         _check(lib().heom_run_scan(self._h, pts.ctypes.data_as(ctypes.c_void_p), len(pts), _dptr(P),
                                    off.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
                                    cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))

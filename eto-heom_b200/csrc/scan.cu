@@ -38,6 +38,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstdlib>
 #include <complex>
 #include <cstring>
@@ -2469,9 +2470,16 @@ int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, co
     rc = staged_status(s, st);
     if (rc) return rc;
   }
-  std::memcpy(P, s.h_P, sizeof(double2) * total);
-  for (long long q = 0; q < 2 * total; q++)
-    if (!std::isfinite(P[q])) { s_err = "non-finite P(t) in the scan: the propagation diverged"; return HEOM_ERR_NUMERIC; }
+  // copy out and check in one pass: a value is finite unless its exponent bits are all set
+  const uint64_t *src = (const uint64_t *)s.h_P;
+  uint64_t *dst = (uint64_t *)P;
+  uint64_t bad = 0;
+  for (long long q = 0; q < 2 * total; q++) {
+    const uint64_t v = src[q];
+    dst[q] = v;
+    bad |= (uint64_t)((v & 0x7ff0000000000000ull) == 0x7ff0000000000000ull);
+  }
+  if (bad) { s_err = "non-finite P(t) in the scan: the propagation diverged"; return HEOM_ERR_NUMERIC; }
   return 0;
 }
 
