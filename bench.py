@@ -218,6 +218,31 @@ def run_reference_arm(a):
 C1_KEY = os.path.join(ROOT, "tests", "golden", "keys", "c1_fmo.key")
 
 
+def c3_record(heom, device: int) -> dict:
+    """Config 3, the precision study: the 12-site chain (single-excitation manifold, N = 13,
+    2925 ADOs), linear response (pulse 3 only) over 6001 RK4 steps, FP32-bulk contractions
+    on FP64 state against the bit-exact FP64 path and the FP64 staged path."""
+    from heomtest import rel_err
+
+    k = os.path.join(ROOT, "tests", "golden", "keys", "c3_chain.key")
+    out = {}
+    P = {}
+    for prec in ("fp64-exact", "fp64", "fp32-bulk"):
+        prob = heom.Problem.from_key(k, single_manifold=True)
+        prob.prepare_sample()
+        plan = heom.Plan(prob, prec, device=device)
+        plan.run_traj(0, 0, 1)
+        t0 = time.perf_counter()
+        P[prec] = plan.run_traj(0, 0, 1)
+        out[prec.replace("-", "_") + "_ms_per_step"] = 1e3 * (time.perf_counter() - t0) / 6001
+    inf = heom.Problem.from_key(k, single_manifold=True).info
+    out.update({"workload": f"c3 chain: N={inf.sys_size}, {inf.n_ado} ADOs, 6001 RK4 steps, linear response",
+                "fp32_bulk_vs_fp64_exact_max_rel_err": rel_err(P["fp32-bulk"], P["fp64-exact"]),
+                "fp32_bulk_vs_fp64_staged_max_rel_err": rel_err(P["fp32-bulk"], P["fp64"]),
+                "fp64_staged_vs_fp64_exact_max_rel_err": rel_err(P["fp64"], P["fp64-exact"])})
+    return out
+
+
 def large_n_record(heom, device: int, fp32_peak: float) -> dict:
     """The FMO aggregate (N = 29 with the two-exciton manifold, K = 14, L = 3, 680 ADOs):
     one 2DES point, pulses at 50/150/250 fs, propagated to 300 fs (601 RK4 steps), on
@@ -455,6 +480,7 @@ def run_ours(a):
         cpu_val, kind, wall, _ = reference_cpu(rows, cores, cores)
         clocks = clk.summary()
         large_n = large_n_record(heom, local, peak)
+        precision_c3 = c3_record(heom, local)
         adjoint = adjoint_record(heom, local)
         # cold-sample e2e: a new disorder/orientation sample before every scan
         # (heom_problem_prepare_sample + heom_plan_update + heom_run_scan), so the per-sample
@@ -514,6 +540,7 @@ def run_ours(a):
                                        "scan as points per second over the sample"},
             "clocks": clocks,
             "large_n": large_n,
+            "precision_c3": precision_c3,
             "adjoint_c4": adjoint,
         }
         if averaged:
