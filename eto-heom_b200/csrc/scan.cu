@@ -885,7 +885,15 @@ std::string scan_describe(const ScanState &s) {
                                   : "elements (generic form)",
                 s.smem, s.grid,
                 s.tune_ms > 0 ? " (autotuned)" : "");
-  return b;
+  std::string d = b;
+  if (s.staged) { // what heom_run_scan runs: the staged job queue; the shape above is the single pass
+    std::snprintf(b, sizeof b,
+                  "staged: job-queue kernel of %d CTAs x %d threads (one per slot ADO block), %zu B smem, "
+                  "then the dual-tail kernel; single pass: ",
+                  s.sl_grid, s.sl_threads, s.sl_smem);
+    d = b + d;
+  }
+  return d;
 }
 
 cudaError_t scan_enqueue(const ScanState &s, const heom_scan_point *d_pts, int n, double *d_P,
