@@ -444,10 +444,12 @@ def run_ours(a):
     if rank == 0:
         # e2e through the host-buffer C ABI
         e2e_t = []
+        host_out = np.empty(max(tot, 1), dtype=np.complex128)  # the caller's output, reused across scans
         for s in range(max(2, min(a.steps, 5))):
             t0 = time.perf_counter()
-            r32 = plan.run_scan(pts, (pts, off, cnt, tot))
+            r32 = plan.run_scan(pts, (pts, off, cnt, tot), out=host_out)
             e2e_t.append(time.perf_counter() - t0)
+        r32 = heom.ScanResult(r32.P.copy(), r32.offsets, r32.counts)
         e2e_val = n / float(np.mean(e2e_t[1:] if len(e2e_t) > 1 else e2e_t))
         # accuracy gate: FP32-bulk vs the FP64 scan path on the full scan
         r64 = heom.Plan(prob, "fp64", device=local, max_points=n).run_scan(pts, (pts, off, cnt, tot))
@@ -491,7 +493,7 @@ def run_ours(a):
             t0 = time.perf_counter()
             prob.prepare_sample()
             plan.update()
-            plan.run_scan(pts, (pts, off, cnt, tot))
+            plan.run_scan(pts, (pts, off, cnt, tot), out=host_out)
             cold_t.append(time.perf_counter() - t0)
         warm_s = float(np.mean(e2e_t[1:] if len(e2e_t) > 1 else e2e_t))
         e2e_cold = {"value": n / float(np.mean(cold_t)), "unit": UNIT,

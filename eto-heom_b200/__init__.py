@@ -295,9 +295,17 @@ class Plan:
                                       cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(tot)))
         return pts, off, cnt, int(tot.value)
 
-    def run_scan(self, points: np.ndarray, layout=None) -> ScanResult:
+    def run_scan(self, points: np.ndarray, layout=None, out: np.ndarray | None = None) -> ScanResult:
+        """heom_run_scan.  out: an optional complex128 buffer of at least the layout's total
+        to write P into (reused across calls, it saves the allocation and first touch of a
+        new output array); the result's P is a view of it."""
         pts, off, cnt, tot = layout if layout is not None else self.scan_layout(points)
-        P = np.empty(max(tot, 1), dtype=np.complex128)  # every value is written by the call
+        if out is not None:
+            if out.dtype != np.complex128 or not out.flags.c_contiguous or out.size < max(tot, 1):
+                raise ValueError("out must be a contiguous complex128 array of at least the scan's total points")
+            P = out
+        else:
+            P = np.empty(max(tot, 1), dtype=np.complex128)  # every value is written by the call
         _check(lib().heom_run_scan(self._h, pts.ctypes.data_as(ctypes.c_void_p), len(pts), _dptr(P),
                                    off.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
                                    cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))

@@ -185,3 +185,16 @@ def test_staged_replay_matches_planned_run():
     fresh = heom.Plan(pb, "fp32-bulk", max_points=len(rows)).run_scan(pts)
     assert np.array_equal(second.P, fresh.P)
     assert not np.array_equal(second.P, first.P)
+
+
+def test_scan_into_caller_buffer(setup):
+    heom, prob = setup
+    rows = scan_geometry()[:6]
+    plan = heom.Plan(prob, "fp32-bulk", max_points=len(rows))
+    lay = plan.scan_layout(heom.make_points(rows))
+    want = plan.run_scan(lay[0], lay)
+    buf = np.full(lay[3] + 5, np.nan, dtype=np.complex128)
+    got = plan.run_scan(lay[0], lay, out=buf)
+    assert np.shares_memory(got.P, buf) and np.array_equal(got.P, want.P)
+    with pytest.raises(ValueError):
+        plan.run_scan(lay[0], lay, out=np.zeros(lay[3] - 1, dtype=np.complex128))
