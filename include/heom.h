@@ -148,7 +148,10 @@ int heom_run_2des(heom_plan *plan, double *P, double *p_traj, int cap, int *n_ou
  * the queue (shared stages, pulse windows and jumps) and the pulse-free tail kernel;
  * the per-sample block powers are formed on the first run after a sample changes.
  * With heom_opts.single_pass = 1 the scan is one persistent kernel launch (after an
- * ordering kernel) replayed from a CUDA graph.  Output of point i: counts[i] combined
+ * ordering kernel) replayed from a CUDA graph.  A staged plan keeps its last job plan:
+ * a scan with the same points and offsets into the same output buffer, on a sample of
+ * the same structure (heom_plan_update between disorder samples), skips the host
+ * planning and only resets the queue before its launches.  Output of point i: counts[i] combined
  * P points at P + 2*offsets[i].  heom_scan_layout fills counts/offsets and returns
  * the total number of complex points through *total. */
 typedef struct { double tau1, tau2, tau3; float t_end; int flags; } heom_scan_point;
