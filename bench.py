@@ -278,6 +278,8 @@ def large_n_record(heom, device: int, fp32_peak: float) -> dict:
     Px, tx = timed(px)
     pb = heom.Plan(prob, "fp32-bulk", device=device)
     Pb, tb = timed(pb, trajectories=False)
+    p64 = heom.Plan(prob, "fp64", device=device)
+    P64, t64 = timed(p64, trajectories=False)
     ax = F * 3 * steps / tx / 1e12
     ab = F * 4 * steps / tb / 1e12
     return {
@@ -289,7 +291,12 @@ def large_n_record(heom, device: int, fp32_peak: float) -> dict:
                                "ceiling is half the FMA peak; launch: " + px.describe()},
         "fp32_bulk": {"ms_per_step": tb / steps * 1e3, "tflops": ab, "peak_fp32_fma_tflops": fp32_peak,
                       "frac": ab / fp32_peak, "rel_err_vs_exact": rel_err(Pb, Px),
+                      "rel_err_vs_fp64_staged": rel_err(Pb, P64),
                       "note": "four mixed-difference components per step (general-size staged path)"},
+        "fp64_staged": {"ms_per_step": t64 / steps * 1e3, "tflops": F * 4 * steps / t64 / 1e12,
+                        "peak_fp64_fma_tflops": fp64_peak, "frac": F * 4 * steps / t64 / 1e12 / fp64_peak,
+                        "fp32_bulk_speedup": t64 / tb,
+                        "note": "the same four components with FP64 contractions"},
     }
 
 
