@@ -1639,6 +1639,7 @@ __global__ void __launch_bounds__(kDualRowThreads) dual_rows_kernel(int cells, c
 // in registers run the chain on the host.
 static int dual_rows(ScanState &s, int rows, cudaStream_t st) {
   const int cells = s.tail_n * s.n_ado;
+  s.dual_launched = false;
   if (cells <= kDualRowThreads * kDualRowCells && cells > 0) {
     cudaError_t e = cudaSuccess;
     const size_t row_bytes = sizeof(double2) * (size_t)cells;
@@ -1694,7 +1695,7 @@ static int dual_rows(ScanState &s, int rows, cudaStream_t st) {
                                                                 (double2 *)s.d_W, s.W_dev_rows, rows);
         e = cudaGetLastError();
       }
-      if (e == cudaSuccess) { s.W_dev_rows = rows; s.staged_launches++; }
+      if (e == cudaSuccess) { s.W_dev_rows = rows; s.staged_launches++; s.dual_launched = true; }
     }
     if (e == cudaSuccess) e = cudaEventRecord(s.ev_join, s.aux);
     if (e == cudaSuccess && s.dual_pos_dirty) {
@@ -1807,6 +1808,11 @@ static long long gap_steps(const ScanState &s, const TimeGrid &g, const SlotJob 
 static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, double *d_P, const long long *offsets,
                            cudaStream_t st) {
   s.rp.valid = false;
+  if (s.rp_graph) { // its last launch may still run
+    cudaStreamSynchronize(st);
+    cudaGraphExecDestroy(s.rp_graph);
+    s.rp_graph = nullptr;
+  }
   const int NN = s.N * s.N;
   const size_t snap_elems = (size_t)NN * s.n_ado; // double2 per state
   std::vector<PtPlan> pl(n);
@@ -2303,11 +2309,24 @@ static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, doub
 // A repeat of the last planned scan (same points, offsets, output buffer and sample): the
 // job tables, saves and tail points on the device are still those of that plan, so only
 // the per-run state is reset before the two launches.
-static int staged_replay(ScanState &s, cudaStream_t st) {
+// The per-run part of a replay on st: reset the queue counter and the flags, then the
+// slot kernel and the tail kernel.
+static cudaError_t replay_enqueue(const ScanState &s, const SlotArgs &a, const DualArgs &da, cudaStream_t st) {
   const ScanState::Replay &r = s.rp;
   cudaError_t e = cudaMemsetAsync(s.d_counter, 0, sizeof(int), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.d_flags, 0, sizeof(int) * r.nflags, st);
-  if (e != cudaSuccess) { s_err = std::string("staged scan reset: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  if (e != cudaSuccess) return e;
+  slot_kernel(s.precision)<<<r.grid, s.sl_threads, s.sl_smem, st>>>(a);
+  e = cudaGetLastError();
+  if (e == cudaSuccess && r.tails) {
+    scan_tail_dual<<<r.tail_grid, kDualThreads, r.tail_smem, st>>>(da);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+static int staged_replay(ScanState &s, cudaStream_t st) {
+  const ScanState::Replay &r = s.rp;
   if (r.jpow_use > 0) { // prepared for this sample already: no work unless it was dropped
     const int rc = jump_powers(s, r.jpow_use, st);
     if (rc) return rc;
@@ -2320,6 +2339,43 @@ static int staged_replay(ScanState &s, cudaStream_t st) {
   std::memcpy(&a, r.a, sizeof a);
   a.jtab = (const int *)s.d_jtab;
   a.jpow = (const double2 *)s.d_jpow;
+  DualArgs da;
+  std::memcpy(&da, r.da, sizeof da);
+  da.W = (const double2 *)s.d_W;
+  da.W_rows = s.W_dev_rows;
+  // Steady state (no dual rows formed by this call, so nothing to wait for on the
+  // auxiliary stream): the run is one CUDA graph of the two resets and the two kernels,
+  // captured on the first such replay and launched again while its arguments hold.
+  if (!(r.tails && s.dual_launched)) {
+    const void *key[4] = {a.jtab, a.jpow, da.W, (const void *)(size_t)da.W_rows};
+    if (s.rp_graph && std::memcmp(key, s.rp_graph_key, sizeof key) != 0) {
+      cudaStreamSynchronize(st); // its last launch may still run
+      cudaGraphExecDestroy(s.rp_graph);
+      s.rp_graph = nullptr;
+    }
+    if (!s.rp_graph && cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      cudaGraph_t g = nullptr;
+      const cudaError_t le = replay_enqueue(s, a, da, st);
+      const cudaError_t ce = cudaStreamEndCapture(st, &g);
+      if (le == cudaSuccess && ce == cudaSuccess && cudaGraphInstantiate(&s.rp_graph, g, 0) == cudaSuccess)
+        std::memcpy(s.rp_graph_key, key, sizeof key);
+      else
+        s.rp_graph = nullptr;
+      if (g) cudaGraphDestroy(g);
+    }
+    cudaGetLastError(); // a capture that was refused (e.g. on a stream being captured) runs eagerly below
+    if (s.rp_graph) {
+      const cudaError_t e = cudaGraphLaunch(s.rp_graph, st);
+      if (e != cudaSuccess) { s_err = std::string("staged scan graph launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+      s.staged_launches += r.tails ? 2 : 1;
+      s.err_pending = a.err;
+      s.last_work = r.work;
+      return 0;
+    }
+  }
+  cudaError_t e = cudaMemsetAsync(s.d_counter, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.d_flags, 0, sizeof(int) * r.nflags, st);
+  if (e != cudaSuccess) { s_err = std::string("staged scan reset: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
   slot_kernel(s.precision)<<<r.grid, s.sl_threads, s.sl_smem, st>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess) { s_err = std::string("staged scan launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
@@ -2330,10 +2386,6 @@ static int staged_replay(ScanState &s, cudaStream_t st) {
       e = cudaStreamWaitEvent(st, s.ev_join, 0);
       if (e != cudaSuccess) { s_err = std::string("tail rows wait: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
     }
-    DualArgs da;
-    std::memcpy(&da, r.da, sizeof da);
-    da.W = (const double2 *)s.d_W;
-    da.W_rows = s.W_dev_rows;
     scan_tail_dual<<<r.tail_grid, kDualThreads, r.tail_smem, st>>>(da);
     e = cudaGetLastError();
     if (e != cudaSuccess) { s_err = std::string("tail launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
@@ -2493,6 +2545,7 @@ int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, co
 
 void scan_release(ScanState &s) {
   if (s.gexec) cudaGraphExecDestroy(s.gexec);
+  if (s.rp_graph) cudaGraphExecDestroy(s.rp_graph);
   if (s.d_snap) cudaFree(s.d_snap);
   if (s.d_flags) cudaFree(s.d_flags);
   if (s.d_tailpts) cudaFree(s.d_tailpts);

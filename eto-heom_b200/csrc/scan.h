@@ -98,6 +98,9 @@ struct ScanState {
   // output buffer, snapshot buffer and sample structure are unchanged; the kernel arguments are
   // kept as bytes (SlotArgs, DualArgs of scan_slots.cuh)
   std::vector<int> structure;    // what the planner reads of the sample (scan_upload_system)
+  bool dual_launched = false;    // the last dual_rows call launched the chain kernel
+  cudaGraphExec_t rp_graph = nullptr; // a steady-state replay as one graph (staged_replay)
+  const void *rp_graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
   struct Replay {
     bool valid = false, tails = false;
     int n = 0, grid = 0, jpow_use = 0, kmax = 0, tail_grid = 0;

@@ -151,7 +151,9 @@ int heom_run_2des(heom_plan *plan, double *P, double *p_traj, int cap, int *n_ou
  * ordering kernel) replayed from a CUDA graph.  A staged plan keeps its last job plan:
  * a scan with the same points and offsets into the same output buffer, on a sample of
  * the same structure (heom_plan_update between disorder samples), skips the host
- * planning and only resets the queue before its launches.  Output of point i: counts[i] combined
+ * planning and only resets the queue before its launches; once the sample's dual rows
+ * exist, that run is one CUDA graph (captured on its first use, launched after).  Output
+ * of point i: counts[i] combined
  * P points at P + 2*offsets[i].  heom_scan_layout fills counts/offsets and returns
  * the total number of complex points through *total. */
 typedef struct { double tau1, tau2, tau3; float t_end; int flags; } heom_scan_point;

@@ -174,11 +174,13 @@ def test_staged_replay_matches_planned_run():
     plan = heom.Plan(pa, "fp32-bulk", max_points=len(rows))
     first = plan.run_scan(pts)
     work = plan.scan_work
-    again = plan.run_scan(pts)                    # replayed
-    assert np.array_equal(first.P, again.P) and plan.scan_work == work
+    again = plan.run_scan(pts)                    # replayed: captured into a CUDA graph
+    thrice = plan.run_scan(pts)                   # the graph launched again
+    assert np.array_equal(first.P, again.P) and np.array_equal(first.P, thrice.P) and plan.scan_work == work
     pa.prepare_sample()
     plan.update()
-    second = plan.run_scan(pts)                   # replayed on the new sample
+    second = plan.run_scan(pts)                   # replayed on the new sample (new dual rows: no graph)
+    assert np.array_equal(plan.run_scan(pts).P, second.P)   # and as a graph again
     pb = heom.Problem.from_key(key("c0_dimer.key"))
     pb.prepare_sample()
     pb.prepare_sample()
