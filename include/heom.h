@@ -152,10 +152,9 @@ int heom_run_2des(heom_plan *plan, double *P, double *p_traj, int cap, int *n_ou
  * a scan with the same points and offsets into the same output buffer, on a sample of
  * the same structure (heom_plan_update between disorder samples), skips the host
  * planning and only resets the queue before its launches; once the sample's dual rows
- * exist, that run is one CUDA graph (captured on its first use, launched after).  Output
- * of point i: counts[i] combined
- * P points at P + 2*offsets[i].  heom_scan_layout fills counts/offsets and returns
- * the total number of complex points through *total. */
+ * exist, that run is one CUDA graph (captured on its first use, launched after).
+ * Output of point i: counts[i] combined P points at P + 2*offsets[i].  heom_scan_layout
+ * fills counts/offsets and returns the total number of complex points through *total. */
 typedef struct { double tau1, tau2, tau3; float t_end; int flags; } heom_scan_point;
 int heom_scan_layout(const heom_plan *plan, const heom_scan_point *pts, int n,
                      long long *offsets, int *counts, long long *total);
@@ -179,8 +178,9 @@ int heom_plan_sync(heom_plan *plan);
  * plan's next staged scan only, the dependency wait limit becomes wait_ns (default 30 s;
  * at most 60 s), and with unmet != 0 the first job that waits on another job waits for a
  * flag value that no producer sets.  That wait expires after wait_ns: the kernel writes
- * NaN to the job's first records, releases the jobs that wait on it, and the run reports
- * HEOM_ERR_TIMEOUT.  Every memory access stays in bounds; the next run is unaffected. */
+ * NaN to the job's first records and to the states it would have saved, releases the
+ * jobs that wait on it, and the run reports HEOM_ERR_TIMEOUT.  Every memory access stays
+ * in bounds; the next run plans afresh and is unaffected. */
 int heom_plan_inject_wait_fault(heom_plan *plan, unsigned long long wait_ns, int unmet);
 
 /* Delay scan that performs no device allocation, for callers that cannot let a library
