@@ -1,6 +1,6 @@
 // General-size propagation path (HEOM_FP64 / HEOM_FP32_BULK for any N): host state.
 //
-// The state of a batch of points lives in global memory (L2-resident for the BASELINE
+// The state of a batch of points lives in global memory (L2-resident for the configured
 // sizes): one kernel launch per Horner stage over (ADO tile, component, point), with
 // the same arithmetic as the shared-memory scan kernel -- mixed-difference basis for a
 // 2DES point (4 components) or a single pulse mask (1 component), FP64 state and
