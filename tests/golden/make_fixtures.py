@@ -236,6 +236,7 @@ def parse_driver_output(text):
 DYNAMICS = ["d_dimer.key", "d_trimer.key"]
 GOLDEN = ["c0_dimer_short.key", "c0_dimer.key", "c4_trimer_short.key", "t_disorder.key",
           "t_ref_example.key", "t_strong.key", "c1_fmo_short.key",
+          "c4_trimer.key",      # config-4 system at 0-1000 fs, 2001 steps
           "c1_fmo_300fs.key",   # ~12 min of CPU (dense N = 29 zgemm)
           "c1_fmo.key"]         # ~2 h 20 min of CPU (4001 steps)
 
@@ -405,7 +406,7 @@ def write_truth(workers=None):
     write_truth_keys(workers)
 
 
-TRUTH_KEYS = ["c0_dimer_short.key", "c4_trimer_short.key", "t_disorder.key"]
+TRUTH_KEYS = ["c0_dimer_short.key", "c4_trimer_short.key", "t_disorder.key", "c4_trimer.key"]
 
 
 def write_truth_keys(workers=None):

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 SMEM_KEYS = ["c0_dimer_short.key", "t_disorder.key", "t_ref_example.key", "t_strong.key"]
 # c1_fmo_300fs: the 7-site FMO aggregate (N = 29, 680 ADOs) through all three pulse
 # windows, 601 RK4 steps, against the reference build run here for ~12 min of CPU.
-STAGED_KEYS = ["c4_trimer_short.key", "c1_fmo_short.key", "c1_fmo_300fs.key"]
+STAGED_KEYS = ["c4_trimer_short.key", "c4_trimer.key", "c1_fmo_short.key", "c1_fmo_300fs.key"]
 
 
 def test_exact_full_fmo_bit_identical():

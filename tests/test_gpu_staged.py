@@ -103,3 +103,20 @@ def test_run_with_no_records(tmp_path, precision):
     assert prob.info.n_record == 0
     P, tr = heom.Plan(prob, precision).run_2des()
     assert len(P) == 0 and all(len(t) == 0 for t in tr)
+
+
+def test_trimer_full_2des_vs_truth():
+    """The config-4 trimer (N = 7, 210 ADOs) over 0-1000 fs (2001 steps, pulses at 50,
+    150 and 350 fs) on the general-size staged path, against the binary128 truth; the
+    reference build's own combined output is printed beside it."""
+    heom = load_pkg()
+    true = np.load(os.path.join(REF, "truth_c4_trimer.npz"))["combined"]
+    _, comb_ref = golden("c4_trimer.key")
+    errs = {}
+    for prec, tol in (("fp64", 1e-10), ("fp32-bulk", FP32_TOL)):
+        _, plan = _plan(heom, "c4_trimer.key", prec)
+        P, _ = plan.run_2des(trajectories=False)
+        errs[prec] = rel_err(P, true)
+        assert len(P) == len(true) and errs[prec] <= tol
+    print(f"\ntrimer 0-1000 fs vs truth: fp64 staged {errs['fp64']:.2e}, fp32-bulk {errs['fp32-bulk']:.2e}, "
+          f"reference build {rel_err(comb_ref, true):.2e}")
