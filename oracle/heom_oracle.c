@@ -994,3 +994,26 @@ int ho_2des_q(ho_problem *p, int max_steps, double *P, int cap, int *npts, doubl
   free(q);
   return 0;
 }
+
+/* One trajectory of the first sample in binary128, each recorded value split into a
+ * double pair (hi, lo) with hi + lo equal to it to ~1e-32: the trajectories of a large
+ * system can run in separate processes and still be combined exactly. */
+int ho_traj_q_split(ho_problem *p, int nv1, int nv2, int nv3, int max_steps, double *P_hi, double *P_lo, int cap,
+                    int *npts) {
+  rng_set(p, p->seed);
+  ho_prepare_sample(p);
+  qreal *q = (qreal *)calloc(2 * (size_t)cap + 2, sizeof(qreal));
+  if (!q) return -1;
+  int n = 0;
+  if (traj_q(p, nv1, nv2, nv3, max_steps, q, q + cap, cap, &n)) { free(q); return -1; }
+  for (int j = 0; j < (n < cap ? n : cap); j++)
+    for (int c = 0; c < 2; c++) {
+      const qreal v = q[c * cap + j];
+      const double hi = (double)v;
+      P_hi[2 * j + c] = hi;
+      P_lo[2 * j + c] = (double)(v - (qreal)hi);
+    }
+  *npts = n;
+  free(q);
+  return 0;
+}

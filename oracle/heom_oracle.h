@@ -60,6 +60,10 @@ int ho_2des(ho_problem *p, int mode, int max_steps, double *P, int cap, int *npt
  * discrete scheme (~1e-24 relative on the combined output), rounded to double.
  * Same arguments as ho_2des (no mode: the RHS is the structured form). */
 int ho_2des_q(ho_problem *p, int max_steps, double *P, int cap, int *npts, double *traj);
+/* One binary128 trajectory (mask nv1 nv2 nv3) of the first sample, each value as a
+ * (hi, lo) double pair, so that separately run trajectories combine exactly. */
+int ho_traj_q_split(ho_problem *p, int nv1, int nv2, int nv3, int max_steps, double *P_hi, double *P_lo, int cap,
+                    int *npts);
 
 #ifdef __cplusplus
 }

@@ -433,13 +433,54 @@ def write_truth_keys(workers=None):
         print(f"truth_scan_driver: {len(names)} files")
 
 
+TRUTH_SPLIT_KEYS = ["c1_fmo_300fs.key"]   # ~1 h of CPU per trajectory (N = 29, binary128)
+
+
+def _split_values(text):
+    """Rows of `heom_oracle --quad-mask` output as exact (re, im) fractions (hi + lo)."""
+    from fractions import Fraction
+    out = []
+    for line in text.splitlines():
+        if line.startswith("#") or not line.strip():
+            continue
+        a, b, c, d = (float(x) for x in line.split())
+        out.append((Fraction(a) + Fraction(b), Fraction(c) + Fraction(d)))
+    return out
+
+
+def write_truth_split():
+    """Binary128 truth of large keys: the three trajectories run as separate processes
+    (heom_oracle --quad-mask, values as hi/lo double pairs) and are combined exactly,
+    p111 - p110 - p101, before rounding to double (truth_<key>.npz: combined)."""
+    from concurrent.futures import ThreadPoolExecutor
+    exe = os.path.join(ROOT, "oracle", "heom_oracle")
+
+    def run(args):
+        name, mask = args
+        return subprocess.run([exe, os.path.join(KEYS, name), "--quad-mask", mask], check=True,
+                              capture_output=True, text=True).stdout
+
+    for name in TRUTH_SPLIT_KEYS:
+        with ThreadPoolExecutor(3) as ex:
+            outs = list(ex.map(run, [(name, m) for m in ("111", "110", "101")]))
+        t111, t110, t101 = (_split_values(o) for o in outs)
+        comb = np.array([complex(float(a[0] - b[0] - c[0]), float(a[1] - b[1] - c[1]))
+                         for a, b, c in zip(t111, t110, t101)], dtype=np.complex128)
+        np.savez_compressed(os.path.join(REF, "truth_" + name.replace(".key", ".npz")), combined=comb)
+        print(f"truth_{name}: {len(comb)} records")
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--golden", action="store_true", help="golden vectors from the reference build (oracle/_ref)")
     ap.add_argument("--truth", action="store_true", help="binary128 truth vectors (heom_oracle --quad)")
+    ap.add_argument("--truth-split", action="store_true",
+                    help="binary128 truth of the large keys, one process per trajectory (hours)")
     a = ap.parse_args()
     print("\n".join(write_keys()))
     if a.golden:
         write_golden()
     if a.truth:
         write_truth()
+    if a.truth_split:
+        write_truth_split()

@@ -49,3 +49,22 @@ def test_c2_truth_fixture():
           f"min {e.min():.2e}")
     assert all(np.isfinite(w).all() and np.abs(w).max() > 0 for w in want)
     assert e.max() < 0.1
+
+
+def test_split_trajectories_combine_to_the_truth():
+    """heom_oracle --quad-mask runs one binary128 trajectory and prints (hi, lo) pairs; the
+    three masks combined exactly reproduce ho_2des_q's combined output bit for bit."""
+    import os
+    import subprocess
+    import sys
+    from heomtest import ROOT
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_fixtures import _split_values
+    exe = os.path.join(ROOT, "oracle", "heom_oracle")
+    if not os.path.exists(exe):
+        subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "heom_oracle"])
+    outs = [_split_values(subprocess.run([exe, key("t_strong.key"), "--quad-mask", m], check=True,
+                                         capture_output=True, text=True).stdout) for m in ("111", "110", "101")]
+    comb = np.array([complex(float(a[0] - b[0] - c[0]), float(a[1] - b[1] - c[1])) for a, b, c in zip(*outs)])
+    want, _ = oracle().load(key("t_strong.key")).run_2des_truth()
+    assert np.array_equal(comb, want)
