@@ -101,6 +101,8 @@ def lib() -> ctypes.CDLL:
                                  ctypes.POINTER(ctypes.c_longlong)]),
         "heom_run_scan": (I, [P, P, I, D, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(I)]),
         "heom_run_scan_device": (I, [P, P, I, P, P]),
+        "heom_host_alloc": (I, [ctypes.c_size_t, ctypes.POINTER(P)]),
+        "heom_host_free": (I, [P]),
         "heom_plan_describe": (I, [P, ctypes.c_char_p, I]),
         "heom_plan_launch_count": (ctypes.c_longlong, [P]),
         "heom_plan_scan_work": (ctypes.c_longlong, [P]),
@@ -345,6 +347,29 @@ def fma_peak_tflops(device: int = 0, fp64: bool = False) -> float:
     v = ctypes.c_double()
     _check(lib().heom_measure_fma_peak(device, 1 if fp64 else 0, ctypes.byref(v)))
     return float(v.value)
+
+
+class _PinnedBuffer:
+    """Page-locked host memory from heom_host_alloc, exposed to numpy; freed when the
+    last array that uses it goes away."""
+
+    def __init__(self, n: int, dtype: np.dtype):
+        p = ctypes.c_void_p()
+        _check(lib().heom_host_alloc(max(n, 1) * dtype.itemsize, ctypes.byref(p)))
+        self._ptr = p.value
+        self.__array_interface__ = {"shape": (n,), "typestr": dtype.str, "data": (self._ptr, False), "version": 3}
+
+    def __del__(self):
+        if getattr(self, "_ptr", None) and _lib is not None:
+            _lib.heom_host_free(ctypes.c_void_p(self._ptr))
+            self._ptr = None
+
+
+def pinned_empty(n: int, dtype=np.complex128) -> np.ndarray:
+    """A 1-D array of n elements in page-locked host memory (heom_host_alloc).  As the
+    out= buffer of Plan.run_scan it receives P by DMA, checked for Inf/NaN on the device,
+    with no staging copy on the host."""
+    return np.asarray(_PinnedBuffer(int(n), np.dtype(dtype)))
 
 
 def make_points(rows) -> np.ndarray:

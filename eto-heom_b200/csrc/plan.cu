@@ -548,10 +548,25 @@ int heom_run_scan(heom_plan *pl, const heom_scan_point *pts, int n, double *P, c
   for (int i = 0; i < n; i++) total = std::max(total, offsets[i] + counts[i]);
   if (!pl->scan.supported) // hierarchy too large for one CTA: staged path
     return run_sg(pl, 4, nullptr, pts, n, P, offsets, total);
-  const long long before = pl->scan.staged_launches;
+  const long long before = pl->scan.staged_launches, checks = pl->scan.check_launches;
   int rc = heom_dev::scan_run_host(pl->scan, pts, n, P, offsets, total, pl->stream);
   if (rc) return fail(rc, heom_dev::scan_last_error());
   pl->launches += pl->scan.staged ? pl->scan.staged_launches - before : heom_dev::scan_launches_per_run(pl->scan);
+  pl->launches += pl->scan.check_launches - checks;
+  return HEOM_OK;
+}
+
+int heom_host_alloc(size_t bytes, void **ptr) {
+  if (!ptr) return fail(HEOM_ERR_ARG, "bad argument");
+  int rc = heom_dev::host_alloc(bytes, ptr);
+  if (rc) return fail(rc, heom_dev::scan_last_error());
+  return HEOM_OK;
+}
+
+int heom_host_free(void *ptr) {
+  if (!ptr) return HEOM_OK;
+  int rc = heom_dev::host_free(ptr);
+  if (rc) return fail(rc, heom_dev::scan_last_error());
   return HEOM_OK;
 }
 

@@ -43,6 +43,8 @@
 #include <complex>
 #include <cstring>
 #include <functional>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -2495,6 +2497,58 @@ int scan_run_device(ScanState &s, const heom_scan_point *d_pts, int n, double *d
   return 0;
 }
 
+// heom_host_alloc registry: base address -> bytes of every live page-locked buffer.
+namespace {
+std::mutex g_host_mu;
+std::map<uintptr_t, size_t> g_host_bufs;
+} // namespace
+
+int host_alloc(size_t bytes, void **p) {
+  *p = nullptr;
+  cudaError_t e = cudaHostAlloc(p, std::max<size_t>(bytes, 1), cudaHostAllocPortable);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    s_err = std::string("page-locked host buffer: ") + cudaGetErrorString(e);
+    return HEOM_ERR_NOMEM;
+  }
+  std::lock_guard<std::mutex> g(g_host_mu);
+  g_host_bufs[(uintptr_t)*p] = std::max<size_t>(bytes, 1);
+  return 0;
+}
+
+int host_free(void *p) {
+  {
+    std::lock_guard<std::mutex> g(g_host_mu);
+    auto it = g_host_bufs.find((uintptr_t)p);
+    if (it == g_host_bufs.end()) {
+      s_err = "heom_host_free: not a buffer of heom_host_alloc";
+      return HEOM_ERR_ARG;
+    }
+    g_host_bufs.erase(it);
+  }
+  cudaError_t e = cudaFreeHost(p);
+  if (e != cudaSuccess) { s_err = std::string("heom_host_free: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
+  return 0;
+}
+
+bool host_pinned_covers(const void *p, size_t bytes) {
+  const uintptr_t a = (uintptr_t)p;
+  std::lock_guard<std::mutex> g(g_host_mu);
+  auto it = g_host_bufs.upper_bound(a);
+  if (it == g_host_bufs.begin()) return false;
+  --it;
+  return a >= it->first && a - it->first <= it->second && bytes <= it->second - (a - it->first);
+}
+
+// Flags a value of P whose exponent bits are all set (Inf or NaN): the device side of
+// the copy-out straight into a page-locked caller buffer.
+__global__ void p_nonfinite(const unsigned long long *__restrict__ P, long long n, int *bad) {
+  int hit = 0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    hit |= (P[q] & 0x7ff0000000000000ull) == 0x7ff0000000000000ull;
+  if (__syncthreads_or(hit) && threadIdx.x == 0) *bad = 1;
+}
+
 int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, const long long *offsets,
                   long long total, cudaStream_t st) {
   if (!s.supported) { s_err = "scan path unavailable for this problem: " + s.why; return HEOM_ERR_UNSUPPORTED; }
@@ -2508,7 +2562,14 @@ int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, co
     if (e != cudaSuccess) { s_err = "scan output buffer: out of device memory"; return HEOM_ERR_NOMEM; }
     s.P_cap = total;
   }
-  if (total > s.hP_cap) {
+  // P inside a heom_host_alloc buffer: copied there by DMA, checked on the device
+  const bool direct = host_pinned_covers(P, sizeof(double2) * (size_t)total);
+  if (direct && !s.d_bad) {
+    e = cudaMalloc(&s.d_bad, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&s.h_bad, sizeof(int));
+    if (e != cudaSuccess) { s_err = "scan check flag: out of memory"; return HEOM_ERR_NOMEM; }
+  }
+  if (!direct && total > s.hP_cap) {
     if (s.h_P) cudaFreeHost(s.h_P);
     s.h_P = nullptr;
     s.hP_cap = 0;
@@ -2523,12 +2584,27 @@ int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, co
   if (e != cudaSuccess) { s_err = std::string("scan upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
   int rc = s.staged ? staged_run(s, pts, n, s.d_P, offsets, st) : scan_run_device(s, s.d_pts, n, s.d_P, s.d_offsets, st);
   if (rc) return rc;
-  e = cudaMemcpyAsync(s.h_P, s.d_P, sizeof(double2) * total, cudaMemcpyDeviceToHost, st);
+  if (direct) {
+    e = cudaMemsetAsync(s.d_bad, 0, sizeof(int), st);
+    if (e == cudaSuccess) {
+      p_nonfinite<<<2 * 148, 256, 0, st>>>((const unsigned long long *)s.d_P, 2 * total, s.d_bad);
+      e = cudaGetLastError();
+      s.check_launches++;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(P, s.d_P, sizeof(double2) * total, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s.h_bad, s.d_bad, sizeof(int), cudaMemcpyDeviceToHost, st);
+  } else {
+    e = cudaMemcpyAsync(s.h_P, s.d_P, sizeof(double2) * total, cudaMemcpyDeviceToHost, st);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) { s_err = std::string("scan run: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
   if (s.staged) {
     rc = staged_status(s, st);
     if (rc) return rc;
+  }
+  if (direct) {
+    if (*s.h_bad) { s_err = "non-finite P(t) in the scan: the propagation diverged"; return HEOM_ERR_NUMERIC; }
+    return 0;
   }
   // copy out and check in one pass: a value is finite unless its exponent bits are all set
   const uint64_t *src = (const uint64_t *)s.h_P;
@@ -2572,6 +2648,8 @@ void scan_release(ScanState &s) {
   if (s.h_pts) cudaFreeHost(s.h_pts);
   if (s.h_offsets) cudaFreeHost(s.h_offsets);
   if (s.h_P) cudaFreeHost(s.h_P);
+  if (s.d_bad) cudaFree(s.d_bad);
+  if (s.h_bad) cudaFreeHost(s.h_bad);
   s = ScanState();
 }
 

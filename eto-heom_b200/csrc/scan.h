@@ -41,6 +41,10 @@ struct ScanState {
   long long *h_offsets = nullptr;
   double *h_P = nullptr;
   long long hP_cap = 0;
+  // copy-out straight into a caller buffer from heom_host_alloc: the finiteness check
+  // runs on the device (flag d_bad, read back into h_bad)
+  int *d_bad = nullptr, *h_bad = nullptr;
+  long long check_launches = 0;
   // staged scan (scan_slots.cuh): shared R/D2 per (tau1, tau2), per-point pulse-3 window,
   // pulse-free tails two points per CTA
   bool staged = false;           // chosen for heom_run_scan / heom_run_scan_device
@@ -132,6 +136,11 @@ cudaError_t scan_enqueue(const ScanState &s, const heom_scan_point *d_pts, int n
 int scan_upload_system(ScanState &s, const heom::Problem &p, cudaStream_t st);
 int scan_run_host(ScanState &s, const heom_scan_point *pts, int n, double *P, const long long *offsets,
                   long long total, cudaStream_t st);
+// Page-locked host buffers of heom_host_alloc, kept in a registry so that the host-buffer
+// scan entry can recognise an output array that lies inside one of them.
+int host_alloc(size_t bytes, void **p);
+int host_free(void *p);
+bool host_pinned_covers(const void *p, size_t bytes);
 int scan_run_device(ScanState &s, const heom_scan_point *d_pts, int n, double *d_P, const long long *d_offsets,
                     cudaStream_t st);
 // Waits for the stream and returns the status of the last staged run (HEOM_ERR_TIMEOUT

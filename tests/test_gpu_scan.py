@@ -200,3 +200,22 @@ def test_scan_into_caller_buffer(setup):
     assert np.shares_memory(got.P, buf) and np.array_equal(got.P, want.P)
     with pytest.raises(ValueError):
         plan.run_scan(lay[0], lay, out=np.zeros(lay[3] - 1, dtype=np.complex128))
+
+
+def test_scan_into_page_locked_buffer(setup):
+    """An output array from heom_host_alloc receives P by DMA with the Inf/NaN check on
+    the device (one extra launch); the result equals the staged copy-out bit for bit,
+    also at an offset that ends exactly at the buffer's end, and when the buffer is
+    reused."""
+    heom, prob = setup
+    rows = scan_geometry()[:6]
+    plan = heom.Plan(prob, "fp32-bulk", max_points=len(rows))
+    lay = plan.scan_layout(heom.make_points(rows))
+    want = plan.run_scan(lay[0], lay)
+    pinned = heom.pinned_empty(lay[3] + 8)
+    for start in (0, 8, 0):
+        view = pinned[start:start + lay[3]]
+        before = plan.launches
+        got = plan.run_scan(lay[0], lay, out=view)
+        assert np.shares_memory(got.P, pinned) and np.array_equal(got.P, want.P)
+        assert plan.launches - before >= 1

@@ -152,3 +152,14 @@ def test_plan_without_device_fails_loudly(heom):
     with pytest.raises(heom.HeomError) as e:
         heom.Plan(prob)
     assert e.value.code == -4
+
+
+def test_host_free_rejects_foreign_pointers(heom):
+    """heom_host_free frees only buffers of heom_host_alloc: NULL is a no-op, any other
+    pointer is HEOM_ERR_ARG (checked before any CUDA call)."""
+    import ctypes
+    L = heom.lib()
+    assert L.heom_host_free(None) == 0
+    foreign = np.zeros(4)
+    assert L.heom_host_free(ctypes.c_void_p(foreign.ctypes.data)) == -1
+    assert L.heom_host_alloc(16, None) == -1
