@@ -1474,32 +1474,55 @@ static void jump_operator(ScanState &s, const std::vector<double> &sys) {
 // Horner steps of T0 = T4(h L0) and the squarings T0^(2^(j+1)) = (T0^(2^j))^2.  One
 // launch covers every position block: blockIdx.z is the block, whose size and offset
 // (in elements, the same for A, B and C) come from dims / offs; tiles outside a block
-// return at once.
-__global__ void jump_gemm(const int *__restrict__ dims, const long long *__restrict__ offs, double alpha, int ident,
-                          const double2 *__restrict__ A0, const double2 *__restrict__ B0, double2 *__restrict__ C0) {
-  __shared__ double2 As[16][17], Bs[16][17];
+// return at once.  A CTA makes a 32 x 32 tile of C from 16-deep K slices staged in shared
+// memory (A slice stored K-major), each thread a 2 x 2 micro-tile (rows ty, ty + 16,
+// columns tx, tx + 16), so one shared load feeds two complex products.  Every element
+// accumulates over k = 0, 1, ..., d - 1 in order with the same fused operations.
+constexpr int kJumpTile = 32;
+__global__ void __launch_bounds__(256) jump_gemm(const int *__restrict__ dims, const long long *__restrict__ offs,
+                                                 double alpha, int ident, const double2 *__restrict__ A0,
+                                                 const double2 *__restrict__ B0, double2 *__restrict__ C0) {
+  __shared__ double2 As[16][kJumpTile + 1], Bs[16][kJumpTile + 1];
   const int d = dims[blockIdx.z];
-  if ((int)blockIdx.y * 16 >= d || (int)blockIdx.x * 16 >= d) return;
+  const int r0 = (int)blockIdx.y * kJumpTile, c0 = (int)blockIdx.x * kJumpTile;
+  if (r0 >= d || c0 >= d) return;
   const long long o = offs[blockIdx.z];
   const double2 *A = A0 + o, *B = B0 + o;
   double2 *C = C0 + o;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int row = blockIdx.y * 16 + ty, col = blockIdx.x * 16 + tx;
-  double re = 0.0, im = 0.0;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const double2 zero = make_double2(0.0, 0.0);
+  double re[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, im[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
   for (int k0 = 0; k0 < d; k0 += 16) {
-    As[ty][tx] = (row < d && k0 + tx < d) ? A[(size_t)row * d + k0 + tx] : make_double2(0.0, 0.0);
-    Bs[ty][tx] = (k0 + ty < d && col < d) ? B[(size_t)(k0 + ty) * d + col] : make_double2(0.0, 0.0);
+    for (int q = tid; q < 16 * kJumpTile; q += 256) {
+      const int rr = q >> 4, kk = q & 15; // A: consecutive threads read consecutive k of a row
+      As[kk][rr] = (r0 + rr < d && k0 + kk < d) ? A[(size_t)(r0 + rr) * d + k0 + kk] : zero;
+      const int kb = q >> 5, cc = q & 31; // B: consecutive threads read consecutive columns
+      Bs[kb][cc] = (k0 + kb < d && c0 + cc < d) ? B[(size_t)(k0 + kb) * d + c0 + cc] : zero;
+    }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < 16; k++) {
-      const double2 x = As[ty][k], y = Bs[k][tx];
-      re = fma(x.x, y.x, fma(-x.y, y.y, re));
-      im = fma(x.x, y.y, fma(x.y, y.x, im));
+      const double2 x0 = As[k][ty], x1 = As[k][ty + 16], y0 = Bs[k][tx], y1 = Bs[k][tx + 16];
+      re[0][0] = fma(x0.x, y0.x, fma(-x0.y, y0.y, re[0][0]));
+      im[0][0] = fma(x0.x, y0.y, fma(x0.y, y0.x, im[0][0]));
+      re[0][1] = fma(x0.x, y1.x, fma(-x0.y, y1.y, re[0][1]));
+      im[0][1] = fma(x0.x, y1.y, fma(x0.y, y1.x, im[0][1]));
+      re[1][0] = fma(x1.x, y0.x, fma(-x1.y, y0.y, re[1][0]));
+      im[1][0] = fma(x1.x, y0.y, fma(x1.y, y0.x, im[1][0]));
+      re[1][1] = fma(x1.x, y1.x, fma(-x1.y, y1.y, re[1][1]));
+      im[1][1] = fma(x1.x, y1.y, fma(x1.y, y1.x, im[1][1]));
     }
     __syncthreads();
   }
-  if (row < d && col < d)
-    C[(size_t)row * d + col] = make_double2((ident && row == col ? 1.0 : 0.0) + alpha * re, alpha * im);
+#pragma unroll
+  for (int a = 0; a < 2; a++)
+#pragma unroll
+    for (int b = 0; b < 2; b++) {
+      const int row = r0 + ty + 16 * a, col = c0 + tx + 16 * b;
+      if (row < d && col < d)
+        C[(size_t)row * d + col] =
+            make_double2((ident && row == col ? 1.0 : 0.0) + alpha * re[a][b], alpha * im[a][b]);
+    }
 }
 
 // Powers T0^(2^j), j < need, of every jump block on the device (cached per sample).
@@ -1563,7 +1586,7 @@ static int jump_powers(ScanState &s, int need, cudaStream_t st) {
   }
   const int *dims = (const int *)s.d_jdims;
   const long long *offs = (const long long *)((const unsigned char *)s.d_jtab + s.jmeta_offs);
-  const dim3 g((dmax + 15) / 16, (dmax + 15) / 16, nb), t(16, 16);
+  const dim3 g((dmax + kJumpTile - 1) / kJumpTile, (dmax + kJumpTile - 1) / kJumpTile, nb), t(256);
   auto gemm = [&](double alpha, int ident, const double2 *A, const double2 *B, double2 *C) {
     jump_gemm<<<g, t, 0, st>>>(dims, offs, alpha, ident, A, B, C);
   };
