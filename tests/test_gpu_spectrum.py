@@ -64,7 +64,8 @@ def test_spectral_loss_gradient_matches_central_differences():
     loss = sp.spectral_loss(_spectrum(sp, sp.signal_columns(P, off, cnt)), target)
     loss.backward()
     grad = theta.grad.numpy()
-    assert abs(float(loss) - _loss_plain(heom, sp, params, th0, pts, target)) <= 1e-12 * float(loss)
+    lv = float(loss.detach())
+    assert abs(lv - _loss_plain(heom, sp, params, th0, pts, target)) <= 1e-12 * lv
 
     def central(i, h):
         d = h * abs(th0[i])

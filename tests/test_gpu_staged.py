@@ -120,3 +120,20 @@ def test_trimer_full_2des_vs_truth():
         assert len(P) == len(true) and errs[prec] <= tol
     print(f"\ntrimer 0-1000 fs vs truth: fp64 staged {errs['fp64']:.2e}, fp32-bulk {errs['fp32-bulk']:.2e}, "
           f"reference build {rel_err(comb_ref, true):.2e}")
+
+
+def test_fmo_2des_vs_truth():
+    """The FMO aggregate (N = 29, 680 ADOs) through all three pulse windows (601 steps) on
+    the general-size staged path, against the binary128 truth (three trajectories run
+    separately and combined exactly); the reference build's own output is printed."""
+    heom = load_pkg()
+    true = np.load(os.path.join(REF, "truth_c1_fmo_300fs.npz"))["combined"]
+    _, comb_ref = golden("c1_fmo_300fs.key")
+    errs = {}
+    for prec, tol in (("fp64", 1e-10), ("fp32-bulk", FP32_TOL)):
+        _, plan = _plan(heom, "c1_fmo_300fs.key", prec)
+        P, _ = plan.run_2des(trajectories=False)
+        errs[prec] = rel_err(P, true)
+        assert len(P) == len(true) and errs[prec] <= tol
+    print(f"\nFMO 0-300 fs vs truth: fp64 staged {errs['fp64']:.2e}, fp32-bulk {errs['fp32-bulk']:.2e}, "
+          f"reference build {rel_err(comb_ref, true):.2e}")

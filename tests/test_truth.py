@@ -68,3 +68,18 @@ def test_split_trajectories_combine_to_the_truth():
     comb = np.array([complex(float(a[0] - b[0] - c[0]), float(a[1] - b[1] - c[1])) for a, b, c in zip(*outs)])
     want, _ = oracle().load(key("t_strong.key")).run_2des_truth()
     assert np.array_equal(comb, want)
+
+
+@pytest.mark.parametrize("name", ["c4_trimer.key", "c1_fmo_300fs.key"])
+def test_large_key_truth_fixture(name):
+    """The binary128 truth of the config-4 trimer (0-1000 fs) and of the FMO aggregate
+    through its three pulse windows (0-300 fs): one combined value per reference record,
+    departing from the reference build's combined output by its rounding noise only."""
+    import os
+    from heomtest import REF
+    want = np.load(os.path.join(REF, "truth_" + name.replace(".key", ".npz")))["combined"]
+    _, comb_ref = golden(name)
+    assert want.shape == comb_ref.shape and np.isfinite(want).all() and np.abs(want).max() > 0
+    noise = rel_err(comb_ref, want)
+    print(f"\n{name}: reference combined vs truth {noise:.2e}")
+    assert 1e-12 < noise < 1e-5
