@@ -281,22 +281,25 @@ def large_n_record(heom, device: int, fp32_peak: float) -> dict:
     Pb, tb = timed(pb, trajectories=False)
     p64 = heom.Plan(prob, "fp64", device=device)
     P64, t64 = timed(p64, trajectories=False)
+    # the binary128 truth of this point (the same key as tests/golden/keys/c1_fmo_300fs.key)
+    truth_c1 = np.load(os.path.join(ROOT, "tests", "golden", "ref", "truth_c1_fmo_300fs.npz"))["combined"]
     ax = F * 3 * steps / tx / 1e12
     ab = F * 4 * steps / tb / 1e12
     return {
         "workload": f"c1 FMO 2DES point: N={inf.sys_size}, {inf.n_ado} ADOs, {links} links, {steps} RK4 steps",
         "flop_per_trajectory_step": F,
         "fp64_exact": {"ms_per_step": tx / steps * 1e3, "tflops": ax, "peak_fp64_fma_tflops": fp64_peak,
-                       "frac": ax / fp64_peak,
-                       "note": "three trajectories per step; bit-exact arithmetic uses no FMA, so its "
-                               "ceiling is half the FMA peak; launch: " + px.describe()},
+                       "frac": ax / fp64_peak, "rel_err_vs_truth": rel_err(Px, truth_c1),
+                       "note": "three trajectories per step; its output is the reference build's, bit for bit, so "
+                               "rel_err_vs_truth is the reference's own rounding noise; bit-exact arithmetic uses no "
+                               "FMA, so its ceiling is half the FMA peak; launch: " + px.describe()},
         "fp32_bulk": {"ms_per_step": tb / steps * 1e3, "tflops": ab, "peak_fp32_fma_tflops": fp32_peak,
                       "frac": ab / fp32_peak, "rel_err_vs_exact": rel_err(Pb, Px),
-                      "rel_err_vs_fp64_staged": rel_err(Pb, P64),
+                      "rel_err_vs_fp64_staged": rel_err(Pb, P64), "rel_err_vs_truth": rel_err(Pb, truth_c1),
                       "note": "four mixed-difference components per step (general-size staged path)"},
         "fp64_staged": {"ms_per_step": t64 / steps * 1e3, "tflops": F * 4 * steps / t64 / 1e12,
                         "peak_fp64_fma_tflops": fp64_peak, "frac": F * 4 * steps / t64 / 1e12 / fp64_peak,
-                        "fp32_bulk_speedup": t64 / tb,
+                        "fp32_bulk_speedup": t64 / tb, "rel_err_vs_truth": rel_err(P64, truth_c1),
                         "note": "the same four components with FP64 contractions"},
     }
 
@@ -464,6 +467,18 @@ def run_ours(a):
         # accuracy gate: FP32-bulk vs the FP64 scan path on the full scan
         r64 = heom.Plan(prob, "fp64", device=local, max_points=n).run_scan(pts, (pts, off, cnt, tot))
         errs = [rel_err(r32.point(i), r64.point(i)) for i in range(n)]
+        # against the binary128 truth of the reference's scheme on a stratified 48-point
+        # subset of this scan (tests/golden/ref/truth_c2.npz, the first sample of the key)
+        truth_acc = None
+        if world == 1:
+            from heomtest import truth
+            t_rows, t_want, t_ref, t_gidx = truth("c2")
+            if all(tuple(rows[int(g)]) == tuple(r) for g, r in zip(t_gidx, t_rows)):
+                truth_acc = {"points": len(t_want),
+                             "fp32_bulk_max_rel_err": max(rel_err(r32.point(int(g)), w) for g, w in zip(t_gidx, t_want)),
+                             "fp64_staged_max_rel_err": max(rel_err(r64.point(int(g)), w) for g, w in zip(t_gidx, t_want)),
+                             "reference_build_max_rel_err": max(rel_err(r, w) for r, w in zip(t_ref, t_want)),
+                             "reference_build_median_rel_err": float(np.median([rel_err(r, w) for r, w in zip(t_ref, t_want)]))}
         # plain FP64 path (bit-exact, one point at a time) on a stratified sample
         tmpl = open(TEMPLATE).read()
         sample_idx = np.linspace(0, n - 1, 8).round().astype(int)
@@ -544,7 +559,8 @@ def run_ours(a):
                                   "plus the time the FP64 work (24N^2 per ADO and stage) needs at the measured "
                                   "FP64 FMA peak, over the measured time")},
             "accuracy": {"fp32_bulk_vs_fp64_max_rel_err": float(max(errs)),
-                         "fp32_bulk_vs_fp64_median_rel_err": float(np.median(errs)), "points_checked": n},
+                         "fp32_bulk_vs_fp64_median_rel_err": float(np.median(errs)), "points_checked": n,
+                         "vs_binary128_truth": truth_acc},
             "plain_fp64": {"value": plain_val, "unit": UNIT, "sample": f"{len(sample_idx)} points, one at a time, "
                            "bit-exact FP64 path, scaled to the scan by RK4 step count",
                            "speedup_of_chosen": value / plain_val},
