@@ -162,14 +162,16 @@ int heom_scan_layout(const heom_plan *plan, const heom_scan_point *pts, int n,
 int heom_run_scan(heom_plan *plan, const heom_scan_point *pts, int n, double *P,
                   const long long *offsets, const int *counts);
 /* Page-locked host memory for heom_run_scan's output (no counterpart in the reference,
- * which prints P).  When P lies inside one buffer from heom_host_alloc, heom_run_scan
- * copies the result into it by DMA and checks it for Inf/NaN on the device.  Into any
- * other memory it copies through the plan's own page-locked staging buffer and checks
- * on the host.  The buffer serves any plan on any device; heom_host_free(NULL) is a
- * no-op and freeing an unknown pointer returns HEOM_ERR_ARG. */
+ * which prints P).  When P lies inside one buffer from heom_host_alloc, a scan on the
+ * batched path (N <= 15) copies the result into it by DMA and checks it for Inf/NaN on
+ * the device.  Into any other memory it copies through the plan's own page-locked
+ * staging buffer and checks on the host.  The general-size path (larger hierarchies)
+ * copies into P directly and checks on the host either way.  The buffer serves any plan
+ * on any device; heom_host_free(NULL) is a no-op and freeing an unknown pointer returns
+ * HEOM_ERR_ARG. */
 int heom_host_alloc(size_t bytes, void **ptr);
 int heom_host_free(void *ptr);
-/* Same with every buffer already in device memory.  A staged scan reads the points and
+/* heom_run_scan with every buffer already in device memory.  A staged scan reads the points and
  * offsets back once to plan its stages (one host synchronisation); a single-pass scan
  * does not synchronise.  Errors found on the device (a dependency wait that expired, a
  * failed device-side check) are deferred: the call returns once the work is queued, and
