@@ -2259,7 +2259,19 @@ static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, doub
       dp.push_back(d);
     }
   }
+  // tiles of at most kTailTP points with one k0 (the points sorted by k0): each tile's
+  // records are one matrix product with shared rows of w
+  std::vector<int2> dtiles;
+  int dmaxc = 0;
   if (!dp.empty()) {
+    std::stable_sort(dp.begin(), dp.end(), [](const DualPoint &x, const DualPoint &y) { return x.k0 < y.k0; });
+    for (size_t i = 0; i < dp.size();) {
+      size_t j = i;
+      while (j < dp.size() && dp[j].k0 == dp[i].k0 && j - i < (size_t)kTailTP) j++;
+      dtiles.push_back(make_int2((int)i, (int)(j - i)));
+      i = j;
+    }
+    for (const DualPoint &d : dp) dmaxc = std::max(dmaxc, d.count);
     int rc = dual_rows(s, kmax, st);
     if (rc) return rc;
   }
@@ -2275,9 +2287,15 @@ static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, doub
         e = cudaStreamWaitEvent(st, s.ev_join, 0);
         if (e != cudaSuccess) { s_err = std::string("tail rows wait: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
       }
-      e = grow<DualPoint>(s.d_tailpts, s.tailpts_cap, dp.size());
+      // the points, then the tiles (int2, 8-byte aligned after the 24-byte points)
+      static_assert(sizeof(DualPoint) % sizeof(int2) == 0, "tile table alignment");
+      const size_t tile_slots = (sizeof(int2) * dtiles.size() + sizeof(DualPoint) - 1) / sizeof(DualPoint);
+      e = grow<DualPoint>(s.d_tailpts, s.tailpts_cap, dp.size() + tile_slots);
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(s.d_tailpts, dp.data(), sizeof(DualPoint) * dp.size(), cudaMemcpyHostToDevice, st);
+      int2 *d_tiles = (int2 *)((DualPoint *)s.d_tailpts + dp.size());
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_tiles, dtiles.data(), sizeof(int2) * dtiles.size(), cudaMemcpyHostToDevice, st);
       if (e != cudaSuccess) { s_err = std::string("tail upload: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
       DualArgs da{};
       da.ne = s.tail_n;
@@ -2287,21 +2305,19 @@ static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, doub
       da.pos = (const int *)s.d_dualpos;
       da.W = (const double2 *)s.d_W;
       da.pts = (const DualPoint *)s.d_tailpts;
+      da.tiles = d_tiles;
       da.NN = s.N * s.N;
       da.W_rows = s.W_dev_rows;
       da.err = (int *)s.d_flags + n;
-      const size_t smem = sizeof(double2) * (size_t)kDualG * s.tail_n * s.n_ado;
-      e = cudaFuncSetAttribute(scan_tail_dual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e == cudaSuccess) {
-        scan_tail_dual<<<(int)((dp.size() + kDualG - 1) / kDualG), kDualThreads, smem, st>>>(da);
-        e = cudaGetLastError();
-      }
+      const dim3 tail_dims((unsigned)dtiles.size(), (unsigned)((dmaxc + kTailTJ - 1) / kTailTJ));
+      scan_tail_dual<<<tail_dims, kTailThreads, 0, st>>>(da);
+      e = cudaGetLastError();
       if (e != cudaSuccess) { s_err = std::string("tail launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
       s.staged_launches++;
       static_assert(sizeof(DualArgs) <= sizeof(s.rp.da), "replay buffer");
       std::memcpy(s.rp.da, &da, sizeof da);
-      s.rp.tail_grid = (int)((dp.size() + kDualG - 1) / kDualG);
-      s.rp.tail_smem = smem;
+      s.rp.tail_grid = (int)tail_dims.x;
+      s.rp.tail_grid_y = (int)tail_dims.y;
     }
   }
   s.last_work = 0;
@@ -2344,7 +2360,7 @@ static cudaError_t replay_enqueue(const ScanState &s, const SlotArgs &a, const D
   slot_kernel(s.precision)<<<r.grid, s.sl_threads, s.sl_smem, st>>>(a);
   e = cudaGetLastError();
   if (e == cudaSuccess && r.tails) {
-    scan_tail_dual<<<r.tail_grid, kDualThreads, r.tail_smem, st>>>(da);
+    scan_tail_dual<<<dim3(r.tail_grid, r.tail_grid_y), kTailThreads, 0, st>>>(da);
     e = cudaGetLastError();
   }
   return e;
@@ -2411,7 +2427,7 @@ static int staged_replay(ScanState &s, cudaStream_t st) {
       e = cudaStreamWaitEvent(st, s.ev_join, 0);
       if (e != cudaSuccess) { s_err = std::string("tail rows wait: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
     }
-    scan_tail_dual<<<r.tail_grid, kDualThreads, r.tail_smem, st>>>(da);
+    scan_tail_dual<<<dim3(r.tail_grid, r.tail_grid_y), kTailThreads, 0, st>>>(da);
     e = cudaGetLastError();
     if (e != cudaSuccess) { s_err = std::string("tail launch: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
     s.staged_launches++;

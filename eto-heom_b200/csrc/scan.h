@@ -46,7 +46,7 @@ struct ScanState {
   int *d_bad = nullptr, *h_bad = nullptr;
   long long check_launches = 0;
   // staged scan (scan_slots.cuh): shared R/D2 per (tau1, tau2), per-point pulse-3 window,
-  // pulse-free tails two points per CTA
+  // pulse-free tails as products with the dual rows
   bool staged = false;           // chosen for heom_run_scan / heom_run_scan_device
   bool rstat = false;            // H couples level 0 to nothing (|0><0| stationary)
   bool r_row0 = false;           // R stays in row 0 and Tr X3 R = 0 (see scan_upload_system)
@@ -63,7 +63,7 @@ struct ScanState {
   long long last_work = 0;       // component-steps propagated by the last staged run
   std::vector<float> t_grid;     // float time of each step (t_start + dt accumulated)
   int tail_n = 0;                // its positions (0: tails run on full blocks)
-  void *d_tailpts = nullptr;     // the tail kernel's points
+  void *d_tailpts = nullptr;     // the tail kernel's points, then its tiles
   size_t tailpts_cap = 0;
   // dual tails (scan_tail_dual): L^T of the pulse-free reduced system (CSR) and its
   // diagonal, w_k rows on the host and the device, the reduced positions
@@ -107,8 +107,8 @@ struct ScanState {
   const void *rp_graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
   struct Replay {
     bool valid = false, tails = false;
-    int n = 0, grid = 0, jpow_use = 0, kmax = 0, tail_grid = 0;
-    size_t nflags = 0, tail_smem = 0;
+    int n = 0, grid = 0, jpow_use = 0, kmax = 0, tail_grid = 0, tail_grid_y = 0;
+    size_t nflags = 0;
     long long work = 0;
     std::vector<int> structure;
     const void *d_P = nullptr, *snap = nullptr;

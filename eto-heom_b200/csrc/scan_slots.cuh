@@ -697,11 +697,16 @@ __global__ void __launch_bounds__(MAXT, 1) scan_slots(SlotArgs a) {
 // the tail records of a point with state q at its window end s3 are
 //   P(s3 + k) = x3^T T^k q = w_k^T q,   w_k = (T^T)^k x3,
 // x3 the readout (Tr X3 . on ADO 0).  The host propagates the dual vectors w_k once per
-// sample in FP64; here each record is one FP64 dot product over the reduced cells.
-// One warp per record, G points per CTA sharing the rows of w.
+// sample in FP64.  A point's records use the rows k0, k0 + stride, k0 + 2 stride, ...,
+// so points with the same k0 share every row, and their records form one complex FP64
+// matrix product P[g][j] = sum_c w_{k0 + j stride}[c] q_g[c] over the reduced cells.
+// The host groups the points by k0 into tiles of at most kTailTP points; a CTA makes
+// one tile's records j0 .. j0 + kTailTJ - 1 from kTailKC-cell slices of the states and
+// of the rows staged in shared memory, each thread a 2 x 2 block (points ty, ty + 16;
+// records tx, tx + 16) accumulated over the cells in order.
 
-constexpr int kDualG = 4;        // points per CTA
-constexpr int kDualThreads = 256;
+constexpr int kTailTP = 32, kTailTJ = 32, kTailKC = 16, kTailThreads = 256;
+static_assert(kTailTJ == kTailTP && kTailKC * kTailTP % kTailThreads == 0, "one staging loop for both slices");
 
 struct DualPoint {
   const double2 *q;  // the point's state at s3, [NN][n_ado] (Q, or Q - R)
@@ -713,47 +718,65 @@ struct DualArgs {
   int ne, nado, stride, n_pts, NN, W_rows;
   const int *pos;        // the reduced positions (r * N + c)
   const double2 *W;      // w_k, [k][cell], cell = e * nado + n
-  const DualPoint *pts;
+  const DualPoint *pts;  // grouped by k0
+  const int2 *tiles;     // (first point, points) of each tile, one k0 per tile
   int *err;              // set when a check fails (the access is skipped)
 };
 
-__global__ void __launch_bounds__(kDualThreads) scan_tail_dual(DualArgs a) {
-  extern __shared__ __align__(16) unsigned char sm[];
-  double2 *q = (double2 *)sm; // [G][cells]
-  __shared__ DualPoint s_pt[kDualG];
-  const int cells = a.ne * a.nado, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int p0 = blockIdx.x * kDualG, G = min(kDualG, a.n_pts - p0);
-  if (tid < G) s_pt[tid] = a.pts[p0 + tid];
-  __syncthreads();
-  for (int t = tid; t < G * cells; t += blockDim.x) {
-    const int g = t / cells, c = t - g * cells, e = c / a.nado, n = c - e * a.nado;
-    const int ps = a.pos[e];
-    if (ps < 0 || ps >= a.NN) { atomicMax(a.err, 5); q[t] = make_double2(0.0, 0.0); continue; }
-    q[t] = __ldcg(s_pt[g].q + (size_t)ps * a.nado + n);
-  }
+__global__ void __launch_bounds__(kTailThreads) scan_tail_dual(DualArgs a) {
+  __shared__ double2 Qs[kTailKC][kTailTP + 1], Ws[kTailKC][kTailTJ + 1];
+  __shared__ DualPoint s_pt[kTailTP];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int2 tile = a.tiles[blockIdx.x];
+  const int np = min(tile.y, kTailTP), j0 = (int)blockIdx.y * kTailTJ;
+  if (tid < np) s_pt[tid] = a.pts[tile.x + tid];
   __syncthreads();
   int jmax = 0;
-  for (int g = 0; g < G; g++) jmax = max(jmax, s_pt[g].count);
-  for (int j = warp; j < jmax; j += blockDim.x >> 5)
-    for (int g = 0; g < G; g++) {
-      const DualPoint &pt = s_pt[g];
-      if (j >= pt.count) continue;
-      if (pt.k0 + j * a.stride >= a.W_rows) {
-        if (lane == 0) atomicMax(a.err, 6);
-        continue;
+  for (int g = 0; g < np; g++) jmax = max(jmax, s_pt[g].count);
+  if (j0 >= jmax) return; // the same for every thread of the CTA
+  const int k0 = s_pt[0].k0, cells = a.ne * a.nado;
+  const double2 zero = make_double2(0.0, 0.0);
+  double re[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, im[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+  for (int c0 = 0; c0 < cells; c0 += kTailKC) {
+    for (int t = tid; t < kTailKC * kTailTP; t += kTailThreads) {
+      const int kc = t % kTailKC, g = t / kTailKC, c = c0 + kc; // consecutive threads: consecutive cells
+      double2 v = zero;
+      if (g < np && c < cells) {
+        const int e = c / a.nado, n = c - e * a.nado, ps = a.pos[e];
+        if (ps < 0 || ps >= a.NN) atomicMax(a.err, 5);
+        else if (s_pt[g].k0 != k0) atomicMax(a.err, 7);
+        else v = __ldcg(s_pt[g].q + (size_t)ps * a.nado + n);
       }
-      const double2 *w = a.W + (size_t)(pt.k0 + j * a.stride) * cells;
-      const double2 *qg = q + (size_t)g * cells;
-      double re = 0.0, im = 0.0;
-      for (int c = lane; c < cells; c += 32) {
-        const double2 x = __ldg(w + c), z = qg[c];
-        re = fma(x.x, z.x, fma(-x.y, z.y, re));
-        im = fma(x.x, z.y, fma(x.y, z.x, im));
+      Qs[kc][g] = v;
+      const int j = j0 + g; // the same slice of the tile's rows (kTailTJ == kTailTP)
+      const long long row = (long long)k0 + (long long)j * a.stride;
+      double2 w = zero;
+      if (j < jmax && c < cells) {
+        if (row >= a.W_rows) atomicMax(a.err, 6);
+        else w = __ldg(a.W + row * cells + c);
       }
-      for (int o = 16; o > 0; o >>= 1) {
-        re += __shfl_xor_sync(0xffffffffu, re, o);
-        im += __shfl_xor_sync(0xffffffffu, im, o);
-      }
-      if (lane == 0) pt.P[j] = make_double2(re, im);
+      Ws[kc][g] = w;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kc = 0; kc < kTailKC; kc++) {
+      const double2 x0 = Ws[kc][tx], x1 = Ws[kc][tx + 16], z0 = Qs[kc][ty], z1 = Qs[kc][ty + 16];
+      re[0][0] = fma(x0.x, z0.x, fma(-x0.y, z0.y, re[0][0]));
+      im[0][0] = fma(x0.x, z0.y, fma(x0.y, z0.x, im[0][0]));
+      re[0][1] = fma(x1.x, z0.x, fma(-x1.y, z0.y, re[0][1]));
+      im[0][1] = fma(x1.x, z0.y, fma(x1.y, z0.x, im[0][1]));
+      re[1][0] = fma(x0.x, z1.x, fma(-x0.y, z1.y, re[1][0]));
+      im[1][0] = fma(x0.x, z1.y, fma(x0.y, z1.x, im[1][0]));
+      re[1][1] = fma(x1.x, z1.x, fma(-x1.y, z1.y, re[1][1]));
+      im[1][1] = fma(x1.x, z1.y, fma(x1.y, z1.x, im[1][1]));
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 2; u++)
+#pragma unroll
+    for (int v = 0; v < 2; v++) {
+      const int g = ty + 16 * u, j = j0 + tx + 16 * v;
+      if (g < np && j < s_pt[g].count && s_pt[g].k0 == k0) s_pt[g].P[j] = make_double2(re[u][v], im[u][v]);
     }
 }
