@@ -1937,35 +1937,37 @@ static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, doub
   }
   std::sort(groups.begin(), groups.end(),
             [](const Group &a, const Group &b) { return a.d2stop - a.first > b.d2stop - b.first; });
-  std::vector<Keyed> qj; // jump jobs: per group a chain through its jumped members in window order
-  int jmax = 0;          // longest jump (steps)
+  // jump jobs: per group one job that carries D2 from the group's base through its jumped
+  // members in window order, saving each member's state and raising its flag on the way
+  // (one CTA walks the chain, so no link waits for another job)
+  std::vector<Keyed> qj;
+  int jmax = 0; // longest single jump (steps)
   for (size_t g = 0; g < groups.size(); g++) {
     const Group &G = groups[g];
-    int base_step = G.d2stop, base_flag = n + 1 + (int)g;
-    const double2 *base = gsnap(g);
+    if (G.jumped.empty()) continue;
+    Keyed K;
+    SlotJob &J = K.job;
+    J = SlotJob{};
+    J.mode = 2;
+    J.first = G.d2stop;
+    J.wait[0] = n + 1 + (int)g;
+    J.wait[1] = J.wait[2] = J.wait[3] = -1;
+    J.wait_val = 1;
+    set_taus(J, 0, pts[G.jumped[0]]);
+    set_taus(J, 1, pts[G.jumped[0]]);
+    for (int h = 0; h < 4; h++) { J.slot[h] = slot_off(); J.rec[h] = rec_off(); }
+    J.slot[0].init = 2;
+    J.slot[0].init_ptr = gsnap(g);
+    int cur = G.d2stop;
     for (int i : G.jumped) { // members are in window order
-      Keyed K;
-      SlotJob &J = K.job;
-      J = SlotJob{};
-      J.mode = 2;
-      J.first = base_step;
-      J.last = pl[i].s2;
-      J.wait[0] = base_flag;
-      J.wait[1] = J.wait[2] = J.wait[3] = -1;
-      J.wait_val = 1;
-      set_taus(J, 0, pts[i]);
-      set_taus(J, 1, pts[i]);
-      for (int h = 0; h < 4; h++) { J.slot[h] = slot_off(); J.rec[h] = rec_off(); }
-      J.slot[0].init = 2;
-      J.slot[0].init_ptr = base;
-      K.saves.push_back(SlotSave{J.last, 0, -1, i, 1, 0, state(i, 1)});
-      K.key = base_step;
-      jmax = std::max(jmax, J.last - J.first);
-      qj.push_back(std::move(K));
-      base_step = pl[i].s2;
-      base_flag = i;
-      base = state(i, 1);
+      const int to = std::max(cur, pl[i].s2);
+      K.saves.push_back(SlotSave{to, 0, -1, i, 1, 0, state(i, 1)});
+      jmax = std::max(jmax, to - cur);
+      cur = to;
     }
+    J.last = cur;
+    K.key = G.d2stop;
+    qj.push_back(std::move(K));
   }
   const size_t solo = std::min<size_t>(groups.size(), (size_t)std::max(0, kSoloGroups));
   for (size_t g = 0; g < groups.size(); g += g < solo ? 1 : 2) {
@@ -2166,9 +2168,17 @@ static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, doub
       if (J.first < 0 || J.last < J.first || J.save_begin < 0 || J.save_end > (int)saves.size()) bad = "job range";
       for (const SlotSpec &z : J.slot)
         if (z.init == 2 && !in_snap(z.init_ptr)) bad = "initial snapshot";
-      if (J.mode == 2) {
-        if (J.save_end != J.save_begin + 1 || !in_snap(J.slot[0].init_ptr)) bad = "jump";
-        if ((long long)(J.last - J.first) >> jpow_use != 0 && J.last > J.first) bad = "jump length";
+      if (J.mode == 2) { // a chain of targets in step order, each jump within the powers
+        if (J.save_end <= J.save_begin || J.save_end > (int)saves.size() || !in_snap(J.slot[0].init_ptr)) bad = "jump";
+        else {
+          int cur = J.first;
+          for (int k = J.save_begin; k < J.save_end; k++) {
+            const int to = saves[k].step;
+            if (to < cur || to > J.last) bad = "jump order";
+            else if ((long long)(to - cur) >> jpow_use != 0) bad = "jump length";
+            cur = to;
+          }
+        }
         if (!s.d_jpow || !s.d_jtab) bad = "jump tables";
       }
     }

@@ -8,8 +8,9 @@
 //   1. per (tau1, tau2) group: R and D2 from t_start until the first two pulses are over,
 //      jumping over the pulse-free gap between them, saving D2 (and R where a member
 //      needs it) at the members' window starts or at the group's jump base;
-//   2. jump jobs (mode 2): D2 carried from the base to each member's window start as
-//      T0^(steps) through the block powers of the pulse-free step map;
+//   2. jump jobs (mode 2), one per group: D2 carried from the group's base through its
+//      jumped members' window starts in step order, each leg T0^(steps) through the
+//      block powers of the pulse-free step map;
 //   3. per point: its pulse-3 window (D2 and Q, or R, D2, D3 and Q), recording P and
 //      saving the state at the window's end.
 // The pulse-free tails after the windows run in scan_tail_dual (below) as FP64 dot
@@ -279,9 +280,10 @@ __device__ double2 *jump_apply(const SlotArgs &a, double2 *x, double2 *y, int de
   return x;
 }
 
-// A jump job (mode 2): the state snapshot slot[0].init_ptr at step `first` carried to step
-// `last` with no field on, as T0^(last - first); the result goes to the job's first save,
-// whose flag is then raised.  sbuf: 2 x n_ado * NN doubles2 of scratch.
+// A jump job (mode 2): the state snapshot slot[0].init_ptr at step `first` carried with no
+// field on through the job's saves in step order (each leg T0^(save.step - previous)); each
+// save gets the state at its step and then raises its flag.  sbuf: 2 x n_ado * NN doubles2
+// of scratch.
 template <int NT>
 __device__ void sl_jump(const SlotArgs &a, const SlotJob &J, double2 *sbuf, int tid, int bs) {
   constexpr int NN = NT * NT;
@@ -293,15 +295,21 @@ __device__ void sl_jump(const SlotArgs &a, const SlotJob &J, double2 *sbuf, int 
     x[e] = __ldcg(J.slot[0].init_ptr + plist[f] * nado + (e - f * nado));
   }
   __syncthreads();
-  x = jump_apply(a, x, sbuf + cells, J.last - J.first, NN, tid, bs);
-  const SlotSave &sv = a.saves[J.save_begin];
-  for (int e = tid; e < cells; e += bs) {
-    const int f = e / nado;
-    __stcg(sv.dst + plist[f] * nado + (e - f * nado), x[e]);
+  // the targets in step order: a group's jumped members, each carried from the previous
+  int cur = J.first;
+  for (int k = J.save_begin; k < J.save_end; k++) {
+    const SlotSave &sv = a.saves[k];
+    if (sv.step < cur && tid == 0) atomicMax(a.err, 8); // planner order violated: no jump back
+    x = jump_apply(a, x, x == sbuf ? sbuf + cells : sbuf, max(0, sv.step - cur), NN, tid, bs);
+    cur = max(cur, sv.step);
+    for (int e = tid; e < cells; e += bs) {
+      const int f = e / nado;
+      __stcg(sv.dst + plist[f] * nado + (e - f * nado), x[e]);
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0 && sv.flag >= 0) atomicMax(a.flags + sv.flag, sv.fval);
   }
-  __threadfence();
-  __syncthreads();
-  if (tid == 0 && sv.flag >= 0) atomicMax(a.flags + sv.flag, sv.fval);
 }
 
 template <typename T, int NT, int MAXT>
