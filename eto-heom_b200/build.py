@@ -38,7 +38,7 @@ UNITS = [
     ("sg.cu", []),
     ("adjoint.cu", []),
 ]
-HEADERS = ["heom_host.h", "kernels.h", "exact.cuh", "scan.h", "scan_pm.cuh", "sg.cuh"]
+HEADERS = ["heom_host.h", "kernels.h", "exact.cuh", "scan.h", "scan_pm.cuh", "scan_slots.cuh", "sg.cuh"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:
