@@ -1467,6 +1467,7 @@ static void jump_operator(ScanState &s, const std::vector<double> &sys) {
   s.jdims.resize(nb);
   for (int b = 0; b < nb; b++) s.jdims[b] = (int)blocks[b].size() * nado;
   s.jpow_n = 0;    // powers must be recomputed for this sample
+  s.jleg_formed = 0;
   s.jL_dirty = true;
 }
 
@@ -1525,9 +1526,11 @@ __global__ void __launch_bounds__(256) jump_gemm(const int *__restrict__ dims, c
     }
 }
 
-// Powers T0^(2^j), j < need, of every jump block on the device (cached per sample).
-// Buffers are kept across samples while the block structure needs no more room.
-static int jump_powers(ScanState &s, int need, cudaStream_t st) {
+// Powers T0^(2^j), j < need, of every jump block on the device (cached per sample), and,
+// when leg > 0, the leg T0^leg as the product of the powers of its set bits, stored after
+// the jpow_cap powers.  Buffers are kept across samples while the block structure needs no
+// more room.
+static int jump_powers(ScanState &s, int need, int leg, cudaStream_t st) {
   cudaError_t e = cudaSuccess;
   const size_t pe = (size_t)s.jpow_elems;
   const int nb = s.jtab[0];
@@ -1556,6 +1559,7 @@ static int jump_powers(ScanState &s, int need, cudaStream_t st) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_jtab, s.h_jmeta.data(), meta, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_jL, s.h_jL.data(), sizeof(double2) * pe, cudaMemcpyHostToDevice, st);
     s.jpow_n = 0;
+    s.jleg_formed = 0;
     s.jL_dirty = false;
   }
   if (e == cudaSuccess && need > s.jpow_cap) {
@@ -1563,7 +1567,8 @@ static int jump_powers(ScanState &s, int need, cudaStream_t st) {
     s.d_jpow = nullptr;
     s.jpow_cap = 0;
     s.jpow_n = 0;
-    e = cudaMalloc(&s.d_jpow, sizeof(double2) * pe * need);
+    s.jleg_formed = 0;
+    e = cudaMalloc(&s.d_jpow, sizeof(double2) * pe * (need + 1)); // the powers, then the leg
     if (e == cudaSuccess) s.jpow_cap = need;
   }
   if (e != cudaSuccess) { s_err = std::string("jump tables: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
@@ -1601,9 +1606,27 @@ static int jump_powers(ScanState &s, int need, cudaStream_t st) {
       gemm(1.0, 0, P + (j - 1) * pe, P + (j - 1) * pe, P + j * pe);
     }
   }
+  s.jpow_n = std::max(s.jpow_n, need);
+  if (leg > 0 && (leg >> s.jpow_n) == 0 && __builtin_popcount((unsigned)leg) >= 2 && s.jleg_formed != leg) {
+    // T0^leg = product of T0^(2^j) over the set bits j of leg (powers commute)
+    double2 *dst = P + (size_t)s.jpow_cap * pe;
+    const double2 *cur = nullptr;
+    int left = __builtin_popcount((unsigned)leg), k = 0;
+    for (int j = 0; (leg >> j) != 0; j++) {
+      if (!((leg >> j) & 1)) continue;
+      const double2 *Pj = P + (size_t)j * pe;
+      if (!cur) {
+        cur = Pj;
+      } else {
+        double2 *out = --left == 1 ? dst : (k++ & 1 ? X1 : X0);
+        gemm(1.0, 0, Pj, cur, out);
+        cur = out;
+      }
+    }
+    s.jleg_formed = leg;
+  }
   e = cudaGetLastError();
   if (e != cudaSuccess) { s_err = std::string("jump powers: ") + cudaGetErrorString(e); return HEOM_ERR_CUDA; }
-  s.jpow_n = std::max(s.jpow_n, need);
   return 0;
 }
 
@@ -2151,12 +2174,32 @@ static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, doub
   int jlong = jmax;
   for (const SlotJob &J : jobs)
     if (J.mode == 0) jlong = std::max(jlong, J.last - J.first);
+  // the most frequent leg of the jump jobs (in a scan, the step between consecutive t2
+  // delays): prepared as one matrix, so each such leg is one product instead of one per
+  // set bit of its step count
+  int jleg = 0;
+  {
+    std::map<int, int> legs;
+    for (const SlotJob &J : jobs) {
+      if (J.mode != 2) continue;
+      int cur = J.first;
+      for (int k = J.save_begin; k < J.save_end; k++) {
+        const int d = saves[k].step - cur;
+        if (d > 0 && __builtin_popcount((unsigned)d) >= 2) legs[d]++;
+        cur = std::max(cur, saves[k].step);
+      }
+    }
+    int best = 1; // a leg used once saves nothing over its own products
+    for (const auto &kv : legs)
+      if (kv.second > best) { best = kv.second; jleg = kv.first; }
+  }
   int jpow_use = 0;
   if (jlong > 0 && !s.jtab.empty()) {
     while ((jlong >> jpow_use) != 0) jpow_use++;
-    const int rc = jump_powers(s, jpow_use, st);
+    const int rc = jump_powers(s, jpow_use, jleg, st);
     if (rc) return rc;
   }
+  if (jpow_use == 0 || s.jleg_formed != jleg) jleg = 0;
   { // every index and pointer the slot kernel will follow, checked against its buffer
     const long long nflags = (long long)n + 1 + (long long)groups.size();
     const double2 *s0 = snap, *s1 = snap + s.snap_cap;
@@ -2182,6 +2225,7 @@ static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, doub
         if (!s.d_jpow || !s.d_jtab) bad = "jump tables";
       }
     }
+    if (jleg && (jleg >> jpow_use) != 0) bad = "jump leg";
     for (const SlotSave &sv : saves) {
       if (sv.flag >= nflags || !in_snap(sv.dst)) bad = "save";
     }
@@ -2248,6 +2292,8 @@ static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, doub
   a.jpow = (const double2 *)s.d_jpow;
   a.jpow_stride = s.jpow_elems;
   a.jpow_n = jpow_use; // prepared for this sample by jump_powers above
+  a.jleg_delta = jleg;
+  a.jleg = jleg ? (const double2 *)s.d_jpow + (size_t)s.jpow_cap * s.jpow_elems : nullptr;
   // the tails' records w_k^T q (scan_tail_dual, G points per CTA): planned here so that
   // the dual rows they need are formed on the auxiliary stream while the slot kernel runs
   int kmax = 0;
@@ -2343,6 +2389,7 @@ static int staged_plan_run(ScanState &s, const heom_scan_point *pts, int n, doub
     s.rp.grid = grid;
     s.rp.nflags = (size_t)n + 1 + groups.size();
     s.rp.jpow_use = jpow_use;
+    s.rp.jleg = jleg;
     s.rp.kmax = kmax;
     s.rp.tails = !dp.empty();
     s.rp.work = s.last_work;
@@ -2379,8 +2426,9 @@ static cudaError_t replay_enqueue(const ScanState &s, const SlotArgs &a, const D
 static int staged_replay(ScanState &s, cudaStream_t st) {
   const ScanState::Replay &r = s.rp;
   if (r.jpow_use > 0) { // prepared for this sample already: no work unless it was dropped
-    const int rc = jump_powers(s, r.jpow_use, st);
+    const int rc = jump_powers(s, r.jpow_use, r.jleg, st);
     if (rc) return rc;
+    if (s.jleg_formed != r.jleg) { s_err = "staged scan replay: jump leg not prepared"; return HEOM_ERR_CUDA; }
   }
   if (r.tails) {
     const int rc = dual_rows(s, r.kmax, st);
@@ -2390,6 +2438,7 @@ static int staged_replay(ScanState &s, cudaStream_t st) {
   std::memcpy(&a, r.a, sizeof a);
   a.jtab = (const int *)s.d_jtab;
   a.jpow = (const double2 *)s.d_jpow;
+  a.jleg = a.jleg_delta ? (const double2 *)s.d_jpow + (size_t)s.jpow_cap * s.jpow_elems : nullptr;
   DualArgs da;
   std::memcpy(&da, r.da, sizeof da);
   da.W = (const double2 *)s.d_W;

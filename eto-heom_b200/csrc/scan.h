@@ -88,7 +88,8 @@ struct ScanState {
   std::vector<double> h_jL;
   long long jpow_elems = 0;
   size_t jblocks = 0;
-  int jpow_n = 0, jpow_cap = 0;
+  int jpow_n = 0, jpow_cap = 0; // d_jpow holds jpow_cap powers and one leg T0^jleg_formed after them
+  int jleg_formed = 0;          // the leg formed for this sample (0: none)
   bool jL_dirty = false;
   void *d_jtab = nullptr, *d_jL = nullptr, *d_jpow = nullptr, *d_jtmp = nullptr, *d_jdims = nullptr;
   size_t jL_cap = 0, jtab_cap = 0, jmeta_offs = 0; // kept across samples while large enough
@@ -107,7 +108,7 @@ struct ScanState {
   const void *rp_graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
   struct Replay {
     bool valid = false, tails = false;
-    int n = 0, grid = 0, jpow_use = 0, kmax = 0, tail_grid = 0, tail_grid_y = 0;
+    int n = 0, grid = 0, jpow_use = 0, jleg = 0, kmax = 0, tail_grid = 0, tail_grid_y = 0;
     size_t nflags = 0;
     long long work = 0;
     std::vector<int> structure;

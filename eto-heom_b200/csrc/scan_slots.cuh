@@ -85,6 +85,8 @@ struct SlotArgs {
   const double2 *jpow;   // T0^(2^j) of every block, jpow_stride elements per power
   long long jpow_stride;
   int jpow_n;            // powers available
+  int jleg_delta;        // > 0: a jump of exactly this many steps is one product with jleg
+  const double2 *jleg;   // T0^jleg_delta of every block, laid out as one power
 };
 
 constexpr int kTailMax = 8;
@@ -231,8 +233,9 @@ __device__ __forceinline__ void jump_rows_wide(const double2 *__restrict__ P, co
 
 // T0^delta applied to the block-ordered state x (the positions of jtab's list, each with
 // its n_ado ADOs; y: scratch of the same size) as one dense block mat-vec per set bit of
-// delta, through the powers T0^(2^j).  Every thread of the CTA calls it; returns the
-// buffer that holds the result.  A failed check (powers not prepared, a block outside a
+// delta, through the powers T0^(2^j), or as one product with T0^jleg_delta when delta is
+// that leg (the step count between consecutive delays of a scan, prepared per sample).
+// Every thread of the CTA calls it; returns the buffer that holds the result.  A failed check (powers not prepared, a block outside a
 // power) skips the access, sets the error word and fills the result with NaN, so that
 // every output depending on it reads NaN.  The checks read only values that are the same
 // for every thread, so all threads take the same branch.
@@ -242,14 +245,15 @@ __device__ double2 *jump_apply(const SlotArgs &a, double2 *x, double2 *y, int de
   const int *np = a.jtab + 1, *pfirst = a.jtab + 1 + nb, *moff = a.jtab + 1 + 2 * nb;
   const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
   bool bad = false;
-  for (int j = 0; (delta >> j) != 0; j++) {
-    if (!((delta >> j) & 1)) continue;
-    if (j >= a.jpow_n) { // powers not prepared: give up (checked error, no access)
+  const bool leg = a.jleg_delta > 0 && delta == a.jleg_delta;
+  for (int j = 0; leg ? j == 0 : (delta >> j) != 0; j++) {
+    if (!leg && !((delta >> j) & 1)) continue;
+    if (!leg && j >= a.jpow_n) { // powers not prepared: give up (checked error, no access)
       if (tid == 0) atomicMax(a.err, 3);
       bad = true;
       break;
     }
-    const double2 *Pj = a.jpow + (size_t)j * a.jpow_stride;
+    const double2 *Pj = leg ? a.jleg : a.jpow + (size_t)j * a.jpow_stride;
     for (int b = 0; b < nb; b++) {
       const int d = np[b] * nado, o = pfirst[b] * nado;
       if ((long long)moff[b] + (long long)d * d > a.jpow_stride || pfirst[b] + np[b] > NN) {
