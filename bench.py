@@ -48,7 +48,7 @@ KEY = os.path.join(ROOT, "tests", "golden", "keys", "c0_dimer.key")
 # `bench.py --profile-run fp32-bulk-full` (profiles/scan_slots_dram_dimer_scan.md):
 # 27,223,040 B read (mostly the FP64 jump powers, read cold: ncu and the bench's L2 flush
 # both start the launch with an empty L2) + 5,175,552 B written (snapshots, P records).
-DRAM_BYTES_PER_SCAN = 27223040.0 + 5175552.0
+DRAM_BYTES_PER_SCAN = 29598208.0 + 6949888.0
 TEMPLATE = os.path.join(ROOT, "tests", "golden", "keys", "c2_dimer_scan.key-tmpl")
 
 
