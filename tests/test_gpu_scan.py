@@ -140,6 +140,27 @@ def test_staged_scan_matches_single_pass(setup, precision, tol):
     assert np.array_equal(Pd, a.P[:lay[3]])
 
 
+def test_staged_jump_chains_match_single_pass(setup):
+    """Whole t2 columns of the delay grid (8 delays 100 fs apart) for a few t1: each
+    (tau1, tau2) group's jump job carries D2 through seven members, and every 200-step
+    leg between consecutive delays is one product with the prepared leg T0^200.  The
+    FP64 staged scan against the FP64 single pass, which steps every point."""
+    heom, prob = setup
+    rows = []
+    for t1 in (0.0, 45.0, 160.0):
+        for t2 in [100.0 * k for k in range(8)]:
+            rows.append((50.0, 50.0 + t1, 50.0 + t1 + t2, 50.0 + t1 + t2 + 400.0))  # rephasing
+            rows.append((50.0 + t1, 50.0, 50.0 + t1 + t2, 50.0 + t1 + t2 + 400.0))  # non-rephasing
+    pts = heom.make_points(rows)
+    staged = heom.Plan(prob, "fp64", max_points=len(rows))
+    single = heom.Plan(prob, "fp64", max_points=len(rows), single_pass=True)
+    a, b = staged.run_scan(pts), single.run_scan(pts)
+    assert np.array_equal(a.counts, b.counts)
+    errs = [rel_err(a.point(i), b.point(i)) for i in range(len(rows))]
+    print(f"jump chains, fp64 staged vs single pass: max {max(errs):.2e}")
+    assert max(errs) <= 1e-11
+
+
 @pytest.mark.parametrize("precision", ["fp32-bulk", "fp64"])
 def test_scan_edge_cases(setup, precision):
     """An empty scan, and a staged scan mixing ordinary points with points that record
